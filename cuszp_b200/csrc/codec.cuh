@@ -1,0 +1,255 @@
+// codec.cuh -- device building blocks of the fused cuSZp block codec for sm_100a.
+//
+// Format (identical bytes to the reference, independent of how work is tiled):
+//   [rate region: one byte per data block]  [payload of block 0][payload of block 1]...
+//   data block = 32 consecutive elements (1D), 8x8 elements of one z-slice (2D,
+//   element k = 8*row + col), or 4x4x4 elements (3D, k = 16*z + 4*y + x).
+//   payload = sign map (W bytes) + `rate` bit-planes of W bytes (W = 4 in 1D, 8 in 2D/3D);
+//   in outlier mode optionally preceded by element 0's magnitude in 1..4 LE bytes.
+//   Reference: src/cuSZp_kernels_1D_f32.cu:31-296 (layout), :1165-1183 (outlier choice).
+//
+// Work decomposition (B200-first, not the reference's): persistent CTAs of 8 warps
+// pull tiles of consecutive data blocks from an atomic ticket; a warp owns one data
+// block at a time with one element per lane (two in 2D/3D), so sign maps are warp
+// ballots and bit-planes come out of one 32x32 register transpose across the warp.
+// Payload offsets come from a single-pass decoupled look-back over tiles.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cuszp {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+
+enum Mode : int { MODE_FIXED = 0, MODE_PLAIN = 1, MODE_OUTLIER = 2 };
+
+// Error bits reported through the workspace error word.
+enum : uint32_t { ERR_LOOKBACK_TIMEOUT = 1u, ERR_CAPACITY = 2u };
+
+// Tile status word: [63:62] = 0 none / 1 aggregate / 2 inclusive prefix, [61:0] value.
+constexpr uint64_t ST_AGG = 1ull << 62;
+constexpr uint64_t ST_INC = 2ull << 62;
+constexpr uint64_t ST_VAL = (1ull << 62) - 1;
+
+// Upper bound on look-back polls before a tile gives up (a few hundred ms).
+constexpr int kSpinLimit = 1 << 21;
+
+// Workspace header; followed by one uint64 status word per tile.
+struct WsHeader {
+    uint32_t ticket;     // next tile to hand out
+    uint32_t done;       // CTAs that finished (last one resets the workspace)
+    uint32_t err;        // sticky error bits, read and cleared by the host
+    uint32_t pad;
+    unsigned long long total;   // true stream length S of the last call
+    unsigned long long pad2[3];
+};
+static_assert(sizeof(WsHeader) == 48, "header layout");
+
+struct Geom {
+    uint64_t nbEle;        // 1D element count
+    uint32_t dx, dy, dz;   // dims.x fastest
+    uint32_t bxn, byn;     // blocks along x and y (2D/3D)
+    uint64_t nblocks;      // data blocks that exist
+    uint64_t rate_bytes;   // size of the rate region
+    uint64_t ntiles;       // tiles handed out (1D: covers the whole rate region)
+};
+
+// ------------------------------------------------------------------ scalar helpers
+
+__device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+__device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+__device__ __forceinline__ uint32_t uabs(int32_t a) { return a < 0 ? 0u - (uint32_t)a : (uint32_t)a; }
+__device__ __forceinline__ int bitlen(uint32_t x) { return 32 - __clz(x); }
+
+// Quantizer of src/cuSZp_kernels_1D_f32.cu:3-20 (f32) and 1D_f64.cu:3-8 (f64):
+//   p = x*r; s = (p >= -0.5) ? 0 : 1; q = rzi(p + 0.5) - s.
+// kFusedQuant selects how p + 0.5 is rounded: as a separately rounded add, or as
+// one fma(x, r, 0.5).  The reference build for sm_100 rounds them separately; the
+// golden vectors' rounding-trap inputs (where the two truncate differently) pin it.
+// The conversion is the same cvt.rzi instruction the reference uses, so NaN and
+// out-of-range products convert identically (f32: NaN -> 0, f64: NaN -> INT_MIN).
+#ifndef CUSZP_FUSED_QUANT
+#define CUSZP_FUSED_QUANT 0
+#endif
+constexpr bool kFusedQuant = CUSZP_FUSED_QUANT != 0;
+
+__device__ __forceinline__ int32_t quantize(float x, float r)
+{
+    float p = __fmul_rn(x, r);
+    int32_t s = (p >= -0.5f) ? 0 : 1;
+    float t = kFusedQuant ? __fmaf_rn(x, r, 0.5f) : __fadd_rn(p, 0.5f);
+    return wsub(__float2int_rz(t), s);
+}
+__device__ __forceinline__ int32_t quantize(double x, double r)
+{
+    double p = __dmul_rn(x, r);
+    int32_t s = (p >= -0.5) ? 0 : 1;
+    double t = kFusedQuant ? __fma_rn(x, r, 0.5) : __dadd_rn(p, 0.5);
+    return wsub(__double2int_rz(t), s);
+}
+
+// Reconstruction ((T)q * eb) * 2 of src/cuSZp_kernels_1D_f32.cu:490.
+__device__ __forceinline__ float dequant(int32_t q, float eb) { return __fmul_rn(__fmul_rn(__int2float_rn(q), eb), 2.0f); }
+__device__ __forceinline__ double dequant(int32_t q, double eb) { return __dmul_rn(__dmul_rn((double)q, eb), 2.0); }
+
+// Streaming loads/stores (touched once).
+__device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ void st_stream(float* p, float v) { __stcs(p, v); }
+__device__ __forceinline__ void st_stream(double* p, double v) { __stcs(p, v); }
+
+// ------------------------------------------------------------------ warp bit transpose
+
+// 32x32 bit-matrix transpose across a warp: on entry lane l holds row l (bit b =
+// M[l][b]); on exit lane p holds column p (bit l = M[l][p]).  5 butterfly stages,
+// each one shuffle, one funnel-free shift select and one LOP3.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane)
+{
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
+                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+        uint32_t y = __shfl_xor_sync(FULL, x, j);
+        const bool up = lane & j;
+        const uint32_t keep = up ? m : ~m;
+        const uint32_t sh = up ? (y >> j) : (y << j);
+        x = (x & keep) | (sh & ~keep);
+    }
+    return x;
+}
+
+// Word with bit l = element l  <->  stored little-endian word whose byte b holds
+// elements 8b..8b+7 most-significant-bit first (the reference's plane/sign bytes).
+__device__ __forceinline__ uint32_t to_stream_word(uint32_t bits) { return __byte_perm(__brev(bits), 0, 0x0123); }
+__device__ __forceinline__ uint32_t from_stream_word(uint32_t w) { return __brev(__byte_perm(w, 0, 0x0123)); }
+
+// ------------------------------------------------------------------ payload sizes
+
+template <int DIM, int MODE>
+__device__ __forceinline__ uint32_t payload_size(uint32_t rb)
+{
+    constexpr uint32_t W = DIM == 1 ? 4u : 8u;
+    if constexpr (MODE != MODE_OUTLIER) {
+        return rb ? W + W * rb : 0u;
+    } else {
+        const uint32_t r = rb & 0x1fu;
+        if (rb & 0x80u) return W + (((rb & 0x60u) >> 5) + 1u) + W * r;
+        return r ? W + W * r : 0u;
+    }
+}
+
+// ------------------------------------------------------------------ tile look-back
+
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t v)
+{
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Exclusive prefix of tile `tile` from its predecessors' published words (warp-wide,
+// 32 predecessors per step).  Every wait is bounded: on timeout the error bit is set
+// and the partial sum returned, so no CTA can hang the GPU.
+__device__ __forceinline__ uint64_t lookback(unsigned long long* status, int64_t tile, uint32_t* err, int lane)
+{
+    uint64_t excl = 0;
+    int64_t base = tile - 1;
+    while (base >= 0) {
+        const int64_t idx = base - lane;
+        unsigned long long w;
+        int spins = 0;
+        while (true) {
+            w = idx >= 0 ? ld_acquire(status + idx) : (unsigned long long)ST_INC;
+            const unsigned pending = __ballot_sync(FULL, (w >> 62) == 0);
+            if (!pending) break;
+            if (++spins > kSpinLimit) {
+                if (lane == 0) atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+                return excl;
+            }
+            __nanosleep(32);
+        }
+        const unsigned inc = __ballot_sync(FULL, (w >> 62) == 2);
+        uint64_t v = w & ST_VAL;
+        if (inc) {
+            const int k = __ffs(inc) - 1;
+            excl += warp_sum64(lane <= k ? v : 0);
+            return excl;
+        }
+        excl += warp_sum64(v);
+        base -= 32;
+    }
+    return excl;
+}
+
+// Last CTA out resets the workspace so the next call finds it zeroed.
+__device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* status, uint64_t ntiles)
+{
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t prev = atomicAdd(&hdr->done, 1u);
+        s_last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        for (uint64_t i = threadIdx.x; i < ntiles; i += blockDim.x) status[i] = 0ull;
+        if (threadIdx.x == 0) {
+            hdr->ticket = 0u;
+            hdr->done = 0u;
+        }
+        __threadfence();
+    }
+}
+
+// CTA-wide tile prefix: warp totals -> tile aggregate -> publish -> look-back.
+// Returns (through shared memory) the tile's exclusive byte offset and each warp's
+// offset inside the tile.  Called by all threads.
+__device__ __forceinline__ void tile_scan(uint32_t warp_total, int64_t tile, uint64_t ntiles,
+                                          unsigned long long* status, WsHeader* hdr, uint64_t rate_bytes,
+                                          uint32_t* s_warp, uint64_t* s_base)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_warp[warp] = warp_total;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = lane < kWarps ? s_warp[lane] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < kWarps; o <<= 1) {
+            uint32_t t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const uint64_t agg = __shfl_sync(FULL, incl, kWarps - 1);
+        __syncwarp();
+        if (lane < kWarps) s_warp[lane] = incl - v;
+        if (lane == 0) st_release(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
+        uint64_t excl = 0;
+        if (tile > 0) {
+            excl = lookback(status, tile, &hdr->err, lane);
+            if (lane == 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
+        }
+        if (lane == 0) {
+            *s_base = excl;
+            if ((uint64_t)tile == ntiles - 1) hdr->total = rate_bytes + excl + agg;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace cuszp

@@ -1,0 +1,218 @@
+// codec_launch.cu -- geometry, grid sizing and dispatch of the 36 fused kernels
+// (f32/f64 x fixed/plain/outlier x 1D/2D/3D, compress and decompress), plus the
+// value-range reduction used for relative error bounds.
+#include "codec_launch.cuh"
+#include "codec_kernels.cuh"
+
+#include <mutex>
+
+namespace cuszp {
+
+int make_problem(Problem& p, int type, int mode, int dim, size_t nbEle, unsigned dx, unsigned dy, unsigned dz)
+{
+    p = Problem{};
+    if (type != 0 && type != 1) return E_ARG;
+    if (mode < 0 || mode > 2) return E_ARG;
+    p.type = type; p.mode = mode; p.dim = dim;
+    Geom& g = p.g;
+    g.nbEle = nbEle;
+    g.dx = dx; g.dy = dy; g.dz = dz;
+    if (dim == 1) {
+        g.nblocks = (nbEle + 31) / 32;
+        g.rate_bytes = ((uint64_t)nbEle + 32767) / 32768 * 32768 / 32;
+        g.ntiles = g.rate_bytes / Tiling<1>::TB;
+        if (g.nblocks > 0xffffffffull) return E_ARG;
+    } else if (dim == 2 || dim == 3) {
+        if (dx == 0 || dy == 0 || dz == 0) return E_ARG;
+        if (dx % 4 != 0) return E_UNSUPPORTED;   // src/cuSZp_kernels_2D_f32.cu:94 float4 rows
+        const uint64_t bs = dim == 2 ? 8 : 4;
+        g.bxn = (uint32_t)((dx + bs - 1) / bs);
+        g.byn = (uint32_t)((dy + bs - 1) / bs);
+        const uint64_t nbz = dim == 2 ? dz : (dz + 3) / 4;
+        g.nblocks = nbz * g.byn * g.bxn;
+        if (g.nblocks > 0xffffffffull) return E_ARG;
+        g.rate_bytes = (g.nblocks + 3) / 4 * 4;
+        g.ntiles = (g.nblocks + Tiling<2>::TB - 1) / Tiling<2>::TB;
+        g.nbEle = (uint64_t)dx * dy * dz;
+    } else {
+        return E_ARG;
+    }
+    return OK;
+}
+
+size_t workspace_bytes(const Problem& p)
+{
+    return sizeof(WsHeader) + sizeof(unsigned long long) * (size_t)(p.g.ntiles ? p.g.ntiles : 1);
+}
+
+size_t max_stream_bytes(const Problem& p)
+{
+    const uint64_t W = p.dim == 1 ? 4 : 8;
+    return (size_t)(p.g.rate_bytes + p.g.nblocks * (W + 4 + 32 * W));
+}
+
+// ------------------------------------------------------------------ dispatch tables
+
+template <typename T, int DIM, int MODE>
+static void* ckernel() { return (void*)compress_kernel<T, DIM, MODE>; }
+template <typename T, int DIM, int MODE>
+static void* dkernel() { return (void*)decompress_kernel<T, DIM, MODE>; }
+
+template <typename T, int DIM>
+static void* pick(bool comp, int mode)
+{
+    if (comp) {
+        switch (mode) {
+            case 0: return ckernel<T, DIM, 0>();
+            case 1: return ckernel<T, DIM, 1>();
+            default: return ckernel<T, DIM, 2>();
+        }
+    }
+    switch (mode) {
+        case 0: return dkernel<T, DIM, 0>();
+        case 1: return dkernel<T, DIM, 1>();
+        default: return dkernel<T, DIM, 2>();
+    }
+}
+
+static void* kernel_for(const Problem& p, bool comp)
+{
+    if (p.type == 0) {
+        if (p.dim == 1) return pick<float, 1>(comp, p.mode);
+        if (p.dim == 2) return pick<float, 2>(comp, p.mode);
+        return pick<float, 3>(comp, p.mode);
+    }
+    if (p.dim == 1) return pick<double, 1>(comp, p.mode);
+    if (p.dim == 2) return pick<double, 2>(comp, p.mode);
+    return pick<double, 3>(comp, p.mode);
+}
+
+// Persistent grid: every SM filled to the kernel's occupancy, never more CTAs than tiles.
+static int grid_for(const void* fn, uint64_t ntiles)
+{
+    static std::mutex mu;
+    static int sms[64] = {0};
+    struct Ent { const void* fn; int dev; int occ; };
+    static Ent cache[256];
+    static int ncache = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int occ = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 64 && sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        for (int i = 0; i < ncache; i++)
+            if (cache[i].fn == fn && cache[i].dev == dev) { occ = cache[i].occ; break; }
+        if (occ == 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, 0);
+            if (occ < 1) occ = 1;
+            if (ncache < 256) cache[ncache++] = Ent{fn, dev, occ};
+        }
+    }
+    const uint64_t want = (uint64_t)(dev < 64 ? sms[dev] : 148) * (uint64_t)occ;
+    return (int)(ntiles < want ? ntiles : want);
+}
+
+static int launch(const Problem& p, bool comp, const void* a0, void* a1, double eb, void* ws, cudaStream_t s)
+{
+    if (p.g.ntiles == 0) return OK;
+    void* fn = kernel_for(p, comp);
+    const int grid = grid_for(fn, p.g.ntiles);
+    WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
+    Geom g = p.g;
+    float ebf = (float)eb, rf = 0.5f / (float)eb;
+    double rd = 0.5 / eb;
+    void* args[6];
+    const void* in_or_cmp = a0;
+    void* out_or_cmp = a1;
+    args[0] = &out_or_cmp;   // placeholder, reassigned below
+    args[1] = &in_or_cmp;
+    args[2] = &g;
+    if (p.type == 0) args[3] = comp ? (void*)&rf : (void*)&ebf;
+    else             args[3] = comp ? (void*)&rd : (void*)&eb;
+    args[4] = &hdr;
+    args[5] = &status;
+    if (comp) { args[0] = &in_or_cmp; args[1] = &out_or_cmp; }
+    cudaError_t e = cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, 0, s);
+    return e == cudaSuccess ? OK : E_CUDA;
+}
+
+int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double eb, void* ws, cudaStream_t s)
+{
+    return launch(p, true, d_in, d_cmp, eb, ws, s);
+}
+
+int launch_decompress(const Problem& p, void* d_out, const uint8_t* d_cmp, double eb, void* ws, cudaStream_t s)
+{
+    return launch(p, false, d_cmp, d_out, eb, ws, s);
+}
+
+// ------------------------------------------------------------------ value range
+
+constexpr int kRangeThreads = 256;
+constexpr int kRangeBlocks = 148 * 4;
+
+size_t range_ws_bytes(size_t) { return sizeof(double) * 2 * (kRangeBlocks + 1) + 16; }
+
+template <typename T>
+__global__ void __launch_bounds__(kRangeThreads)
+range_kernel(const T* __restrict__ in, size_t n, T* __restrict__ partial, unsigned* __restrict__ counter,
+             T* __restrict__ result)
+{
+    T mx = -INFINITY, mn = INFINITY;   // NaN-skipping running extrema
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const T v = __ldcs(in + i);
+        mx = fmax(mx, v);
+        mn = fmin(mn, v);
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+        mn = fmin(mn, __shfl_xor_sync(FULL, mn, o));
+    }
+    __shared__ T smx[kRangeThreads / 32], smn[kRangeThreads / 32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { smx[warp] = mx; smn[warp] = mn; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kRangeThreads / 32; w++) { mx = fmax(mx, smx[w]); mn = fmin(mn, smn[w]); }
+        partial[2 * blockIdx.x] = mx;
+        partial[2 * blockIdx.x + 1] = mn;
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        T gmx = -INFINITY, gmn = INFINITY;
+        for (unsigned b = 0; b < gridDim.x; b++) {
+            gmx = fmax(gmx, ((volatile T*)partial)[2 * b]);
+            gmn = fmin(gmn, ((volatile T*)partial)[2 * b + 1]);
+        }
+        const T first = in[0];
+        if (first != first) { gmx = first; gmn = first; }   // CLI loop starts from element 0
+        result[0] = gmn;
+        result[1] = gmx;
+        *counter = 0u;
+    }
+}
+
+int launch_range(const void* d_in, size_t n, int type, void* d_minmax, void* ws, cudaStream_t s)
+{
+    if (n == 0) return E_ARG;
+    unsigned* counter = reinterpret_cast<unsigned*>(ws);
+    char* part = reinterpret_cast<char*>(ws) + 16;
+    const size_t per_block = 4096;
+    unsigned grid = (unsigned)((n + per_block - 1) / per_block);
+    if (grid > (unsigned)kRangeBlocks) grid = kRangeBlocks;
+    if (grid == 0) grid = 1;
+    if (type == 0)
+        range_kernel<float><<<grid, kRangeThreads, 0, s>>>((const float*)d_in, n, (float*)part, counter, (float*)d_minmax);
+    else
+        range_kernel<double><<<grid, kRangeThreads, 0, s>>>((const double*)d_in, n, (double*)part, counter, (double*)d_minmax);
+    return cudaGetLastError() == cudaSuccess ? OK : E_CUDA;
+}
+
+}  // namespace cuszp

@@ -1,0 +1,158 @@
+#ifndef CUSZP_H
+#define CUSZP_H
+
+/*
+ * cuSZp -- error-bounded lossy compressor for f32/f64 arrays, B200 (sm_100a) build.
+ *
+ * Drop-in for the reference cuSZp interface:
+ *   - enums and the two C-linkage entry points below keep the reference's names,
+ *     values and signatures (reference include/cuSZp.h:20-45, src/cuSZp.cu:4,86),
+ *     so `ctypes.CDLL("libcuSZp.so").cuSZp_compress` binds unchanged;
+ *   - the 36 per-mode C++ entry points (cuSZp/cuSZp_entry_*.h), TimingGPU and the
+ *     *_Yafan file helpers keep the reference's C++ signatures.
+ * The compressed stream is byte-identical to the reference's for the same input,
+ * error bound, mode and dimensionality.
+ *
+ * The extensions at the end (no counterpart in the reference) return a status,
+ * take caller-provided workspace, never synchronize, and report the exact stream
+ * length.
+ */
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#ifdef __cplusplus
+#include <cstddef>
+#include "cuSZp/cuSZp_utility.h"
+#include "cuSZp/cuSZp_timer.h"
+#include "cuSZp/cuSZp_entry_1D_f32.h"
+#include "cuSZp/cuSZp_entry_1D_f64.h"
+#include "cuSZp/cuSZp_entry_2D_f32.h"
+#include "cuSZp/cuSZp_entry_2D_f64.h"
+#include "cuSZp/cuSZp_entry_3D_f32.h"
+#include "cuSZp/cuSZp_entry_3D_f64.h"
+#endif
+#include <stdio.h>
+
+#ifdef __cplusplus
+#define CUSZP_DEFAULT_STREAM = 0
+extern "C" {
+#else
+#define CUSZP_DEFAULT_STREAM
+#endif
+
+typedef enum {
+    CUSZP_DIM_1D = 1, // 1D processing (any array)
+    CUSZP_DIM_2D = 2, // 2D processing: 8x8 blocks of each [dim_y x dim_x] slice
+    CUSZP_DIM_3D = 3  // 3D processing: 4x4x4 blocks
+} cuszp_dim_t;
+
+typedef enum {
+    CUSZP_MODE_FIXED   = 0, // no-delta fixed-length encoding
+    CUSZP_MODE_PLAIN   = 1, // Lorenzo delta + fixed-length encoding
+    CUSZP_MODE_OUTLIER = 2  // Lorenzo delta + outlier-preserving fixed-length encoding
+} cuszp_mode_t;
+
+typedef enum {
+    CUSZP_TYPE_FLOAT  = 0,  // f32
+    CUSZP_TYPE_DOUBLE = 1   // f64
+} cuszp_type_t;
+
+/*
+ * Reference entry points (include/cuSZp.h:38-45 of the reference).
+ * All pointers are device pointers.  dims = {x (fastest), y, z}; 1D ignores dims,
+ * 2D/3D ignore nbEle and need dims.x % 4 == 0.  f64 data uses (double)errorBound.
+ * compress: returns once the stream is complete and *cmpSize holds its length.
+ *   The length reported is the true stream length S (rate region + every block
+ *   payload).  The reference reports less than S for single-CTA launches and,
+ *   in 2D/3D, omits the rate-region padding; cuSZp_reference_cmpsize() gives
+ *   that value when it is wanted.
+ * decompress: returns once d_decData holds the reconstruction.  Blocks encoded
+ *   at rate 0 are written as 0.0 (the reference leaves them untouched and its
+ *   CLI pre-zeroes the output, so results agree).
+ * Errors are printed to stderr; compress then sets *cmpSize = 0.
+ */
+void cuSZp_compress(void* d_oriData, unsigned char* d_cmpBytes,
+                    size_t nbEle, size_t* cmpSize, float errorBound,
+                    cuszp_dim_t dim, uint3 dims, cuszp_type_t type, cuszp_mode_t mode,
+                    cudaStream_t stream CUSZP_DEFAULT_STREAM);
+void cuSZp_decompress(void* d_decData, unsigned char* d_cmpBytes,
+                      size_t nbEle, size_t cmpSize, float errorBound,
+                      cuszp_dim_t dim, uint3 dims, cuszp_type_t type, cuszp_mode_t mode,
+                      cudaStream_t stream CUSZP_DEFAULT_STREAM);
+
+/* ------------------------------------------------------------------ extensions
+ * No counterpart in the reference: it has no error reporting, allocates and frees
+ * scratch on every call (src/cuSZp_entry_1D_f32.cu:29-48) and blocks on a 4-byte
+ * device-to-host copy.  These calls let a pipeline keep buffers resident and stay
+ * asynchronous. */
+
+typedef enum {
+    CUSZP_SUCCESS                = 0,
+    CUSZP_ERROR_INVALID_ARGUMENT = 1,
+    CUSZP_ERROR_UNSUPPORTED      = 2, /* 2D/3D with dims.x % 4 != 0 */
+    CUSZP_ERROR_CUDA             = 3,
+    CUSZP_ERROR_TIMEOUT          = 4, /* a bounded device-side wait gave up */
+    CUSZP_ERROR_WORKSPACE        = 5,
+    CUSZP_ERROR_CAPACITY         = 6
+} cuszp_status_t;
+
+/* Capacity that holds the stream of any input of this geometry. */
+size_t cuSZp_max_compressed_size(size_t nbEle, cuszp_dim_t dim, uint3 dims,
+                                 cuszp_type_t type, cuszp_mode_t mode);
+
+/* Device workspace one compress/decompress call of this geometry needs.  A new
+ * workspace must be zero-filled once; every completed call leaves it zeroed. */
+size_t cuSZp_workspace_size(size_t nbEle, cuszp_dim_t dim, uint3 dims,
+                            cuszp_type_t type, cuszp_mode_t mode);
+
+/* Enqueue compression on `stream` without synchronizing.  The stream length S is
+ * written to *d_cmpSize (a device uint64) when d_cmpSize is non-null.  Calls that
+ * share a workspace must be ordered (same stream or explicit dependencies). */
+int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
+                         float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
+                         cuszp_mode_t mode, void* d_workspace, size_t workspaceBytes,
+                         unsigned long long* d_cmpSize, cudaStream_t stream);
+
+/* Enqueue decompression on `stream` without synchronizing. */
+int cuSZp_decompress_async(void* d_decData, const unsigned char* d_cmpBytes, size_t nbEle,
+                           float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
+                           cuszp_mode_t mode, void* d_workspace, size_t workspaceBytes,
+                           cudaStream_t stream);
+
+/* Synchronize `stream`, then read and clear the workspace's error word:
+ * CUSZP_SUCCESS, or CUSZP_ERROR_TIMEOUT if a device-side wait gave up (the
+ * workspace is re-zeroed so it can be reused). */
+int cuSZp_workspace_check(void* d_workspace, size_t workspaceBytes, cudaStream_t stream);
+
+/* Synchronous forms with a status and the true stream length; workspace is taken
+ * from the device's stream-ordered memory pool. */
+int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
+                      size_t* cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
+                      cuszp_type_t type, cuszp_mode_t mode, cudaStream_t stream);
+int cuSZp_decompress_ex(void* d_decData, const unsigned char* d_cmpBytes, size_t nbEle,
+                        size_t cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
+                        cuszp_type_t type, cuszp_mode_t mode, cudaStream_t stream);
+
+/* The compressed size the reference launcher reports for a stream of length
+ * `streamBytes` (src/cuSZp_entry_1D_f32.cu:42-43, src/cuSZp_entry_2D_f64.cu:46-47). */
+size_t cuSZp_reference_cmpsize(size_t streamBytes, size_t nbEle, cuszp_dim_t dim, uint3 dims,
+                               cuszp_type_t type, cuszp_mode_t mode);
+
+/* Relative error bound as the reference CLI derives it for `-eb rel`
+ * (examples/cuSZp.cpp:176-187 f32, :199-210 f64): rel * (max - min), evaluated in
+ * float (f64: rel * (float)(max - min)); min/max are reduced on the device. */
+int cuSZp_rel_error_bound(const void* d_data, size_t nbEle, cuszp_type_t type, float rel,
+                          float* errorBound, cudaStream_t stream);
+
+/* Device min/max with the CLI's NaN semantics, returned as doubles. */
+int cuSZp_value_range(const void* d_data, size_t nbEle, cuszp_type_t type,
+                      double* minValue, double* maxValue, cudaStream_t stream);
+
+/* Version string of this build. */
+const char* cuSZp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif // CUSZP_H
