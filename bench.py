@@ -1,0 +1,600 @@
+"""Benchmark of the fused cuSZp codec on B200.
+
+One step = compress + decompress of one array resident in HBM (the round trip the
+reference CLI times).  Default workload: 512^3 f32 Gaussian random field,
+outlier mode, 3D processing, relative bound 1e-4 (eb derived once from the value
+range, outside the timed region, as the reference CLI does).
+
+Prints ONE JSON line (rank 0).  `value` is whole-job round-trip throughput in GB/s
+of input bytes (10^9 B/s); `compress` / `decompress` give each kernel's GB/s and
+its HBM roofline fraction; `e2e` is the same metric through the reference-
+compatible C entry points with host buffers (H2D input, D2H stream and
+reconstruction inside the timed region); `cpu_baseline` times the CPU oracle on a
+bounded sample.  `--impl reference` times the CPU oracle as the reference arm
+(the reference has no CPU implementation of the path) and, beside it, the
+reference's own CUDA build compiled for sm_100 on the same GPU.
+
+Multi-GPU: one independent replica per rank (the codec has no exchange step);
+`value` = all ranks' input bytes / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cmp/decmp GB/s & %HBM roofline, bit-exact; batched/served vs plain, p50/p99"
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    # name: (description, dtype, mode, dim, shape (z,y,x) or (n,), eb kind, eb value, generator)
+    "grf512_f32_outlier_3d": ("512^3 f32 GRF P(k)~k^-3 in [-50,50], outlier, 3D, rel 1e-4", "f32", "outlier", 3,
+                              (512, 512, 512), "rel", 1e-4, "grf"),
+    "grf512_f32_outlier_2d": ("512^3 f32 GRF, outlier, 2D slices, rel 1e-4", "f32", "outlier", 2,
+                              (512, 512, 512), "rel", 1e-4, "grf"),
+    "grf512_f32_outlier_1d": ("512^3 f32 GRF, outlier, 1D, rel 1e-4", "f32", "outlier", 1,
+                              (512, 512, 512), "rel", 1e-4, "grf"),
+    "sinusoid_f32_plain_1d": ("2^24 f32 8-sinusoid field + N(0,1e-3), 20% zero runs, plain, 1D, abs 1e-4", "f32",
+                              "plain", 1, (1 << 24,), "abs", 1e-4, "sin"),
+    "uniform8192_f64_fixed_2d": ("1x8192x8192 f64 U[-1,1] with 30% zeros, fixed, 2D, abs 1e-3", "f64", "fixed", 2,
+                                 (1, 8192, 8192), "abs", 1e-3, "uni"),
+}
+DEFAULT = "grf512_f32_outlier_3d"
+ALSO = ["uniform8192_f64_fixed_2d", "sinusoid_f32_plain_1d"]
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def make_input(name, device, seed_offset=0):
+    import torch
+    from cuszp_b200 import datagen
+    desc, dt, mode, dim, shape, ebk, ebv, gen = WORKLOADS[name]
+    tdt = torch.float32 if dt == "f32" else torch.float64
+    if gen == "grf":
+        x = datagen.grf_field(shape, seed=1 + seed_offset, device=device, dtype=tdt)
+    elif gen == "sin":
+        x = datagen.sinusoid_field(shape[0], seed=0 + seed_offset, device=device, dtype=tdt)
+    else:
+        x = datagen.uniform_sparse(shape, seed=2 + seed_offset, device=device, dtype=tdt)
+    return x.contiguous()
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def traffic_summary():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------- GPU arm
+
+def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
+    import torch
+    from cuszp_b200 import codec
+    desc, dt, mode, dim, shape, ebk, ebv, gen = WORKLOADS[name]
+    x = make_input(name, device, seed_offset=rank)
+    lay = codec.Layout.of(x, dim)
+    esz = x.element_size()
+    nbytes = x.numel() * esz
+    eb = codec.rel_error_bound(x, ebv) if ebk == "rel" else ebv
+    cap = codec.max_compressed_size(lay, x.dtype, mode)
+    cmp = torch.empty(cap, dtype=torch.uint8, device=device)
+    out = torch.empty_like(x)
+    size = torch.zeros(1, dtype=torch.int64, device=device)
+    ws = codec.Workspace(device)
+    ws.ensure(codec.workspace_size(lay, x.dtype, mode))
+
+    def step():
+        codec.compress_into(x, cmp, eb, mode, dim, lay.dims, size_out=size, stream=stream, workspace=ws)
+        codec.decompress_into(cmp, out, eb, mode, dim, lay.dims, stream=stream, workspace=ws)
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            step()
+    stream.synchronize()
+    ws.check(stream)
+    S = int(size.item())
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    return_clock = None
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device.index or 0) as clk:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for i in range(steps):
+            ev[i][0].record(stream)
+            codec.compress_into(x, cmp, eb, mode, dim, lay.dims, size_out=size, stream=stream, workspace=ws)
+            ev[i][1].record(stream)
+            codec.decompress_into(cmp, out, eb, mode, dim, lay.dims, stream=stream, workspace=ws)
+            ev[i][2].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return_clock = clk.summary()
+    ws.check(stream)
+    total_ms = t0.elapsed_time(t1)
+    c_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    d_ms = [e[1].elapsed_time(e[2]) for e in ev]
+
+    # correctness of what was timed: FP64 error check on the device
+    err = (x.double() - out.double()).abs()
+    ebd = float(torch.tensor(eb, dtype=torch.float32).double())
+    over_eb = int((err > ebd).sum().item())
+    over_11 = int((err > 1.1 * ebd).sum().item())
+    maxerr = float(err.max().item())
+    del err
+
+    res = {
+        "workload": name, "desc": desc, "n": x.numel(), "dtype": dt, "mode": mode, "dim": dim,
+        "dims": list(lay.dims), "eb": eb, "input_bytes": nbytes, "stream_bytes": S, "cr": nbytes / S,
+        "total_ms": total_ms, "compress_ms": statistics.mean(c_ms), "decompress_ms": statistics.mean(d_ms),
+        "compress_ms_min": min(c_ms), "decompress_ms_min": min(d_ms),
+        "over_eb": over_eb, "over_1.1eb": over_11, "max_err_over_eb": maxerr / ebd if ebd else None,
+        "clocks": return_clock, "launches": 2 * steps,
+    }
+    if measure_e2e:
+        res["e2e"] = run_e2e(x, lay, eb, mode, dim, steps, warmup, S)
+    del x, out, cmp
+    return res
+
+
+def run_e2e(x, lay, eb, mode, dim, steps, warmup, S):
+    """Same round trip through the reference-compatible C entry points (pycuSZp):
+    pinned host input -> H2D -> cuSZp_compress -> D2H stream -> cuSZp_decompress -> D2H
+    reconstruction, all inside the timed region."""
+    import torch
+    from cuszp_b200 import codec, pycuSZp
+    dev = x.device
+    h_in = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    h_in.copy_(x)
+    h_out = torch.empty_like(h_in, pin_memory=True)
+    cap = codec.max_compressed_size(lay, x.dtype, mode)
+    h_cmp = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+    d_in = torch.empty_like(x)
+    d_cmp = torch.empty(cap, dtype=torch.uint8, device=dev)
+    d_out = torch.empty_like(x)
+    api = pycuSZp.cuSZp()
+    t = codec.TYPES[x.dtype]
+    m = codec.MODES[mode]
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        d_in.copy_(h_in, non_blocking=True)
+        size = api.compress(ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(d_cmp.data_ptr()), lay.n, eb,
+                            dim=dim, dims=lay.dims, data_type=t, mode=m, stream=sp)
+        h_cmp[:size].copy_(d_cmp[:size], non_blocking=True)
+        api.decompress(ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_cmp.data_ptr()), lay.n, size, eb,
+                       dim=dim, dims=lay.dims, data_type=t, mode=m, stream=sp)
+        h_out.copy_(d_out, non_blocking=True)
+        return size
+
+    for _ in range(max(1, warmup)):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        size = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1)
+    nbytes = x.numel() * x.element_size()
+    assert size == S, "e2e stream length differs from the device-resident run"
+    return {"value": nbytes * steps / (ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": int(S + nbytes), "wall_s": wall,
+            "path": "pycuSZp -> cuSZp_compress/cuSZp_decompress (C ABI), pinned host buffers"}
+
+
+def cpu_baseline(name, device, sample_slices=None):
+    """The CPU oracle (C restatement, OpenMP over blocks) on a bounded sample."""
+    import numpy as np
+    import torch
+    from cuszp_b200 import codec
+    from oracle import oracle as O
+    desc, dt, mode, dim, shape, ebk, ebv, gen = WORKLOADS[name]
+    x = make_input(name, device)
+    eb = codec.rel_error_bound(x, ebv) if ebk == "rel" else ebv
+    if len(shape) == 3:
+        z = sample_slices or max(4, min(shape[0], (16 << 20) // (shape[1] * shape[2])))
+        xs = x[:z].contiguous()
+        sample = f"first {z} of {shape[0]} z-slices ({xs.numel()} elements)"
+    else:
+        k = min(x.numel(), 16 << 20)
+        xs = x[:k].contiguous()
+        sample = f"first {k} of {x.numel()} elements"
+    lay = codec.Layout.of(xs, dim)
+    h = xs.cpu().numpy().ravel()
+    del x
+    # parity of the GPU codec with the oracle on the sample (bit-exact stream)
+    g_stream = codec.compress(xs, eb, mode, dim=dim, dims=lay.dims).cpu().numpy()
+    best = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        s, _ = O.compress(h, eb, codec.MODES[mode], dim, lay.dims)
+        t1 = time.perf_counter()
+        O.decompress(s, lay.n, h.dtype, eb, codec.MODES[mode], dim, lay.dims)
+        t2 = time.perf_counter()
+        if best is None or (t2 - t0) < best[0]:
+            best = (t2 - t0, t1 - t0, t2 - t1)
+    nb = h.nbytes
+    return {"value": nb / best[0] / 1e9, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+            "sample": sample, "compress_gbs": nb / best[1] / 1e9, "decompress_gbs": nb / best[2] / 1e9,
+            "stream_identical_to_gpu": bool(np.array_equal(g_stream, s))}
+
+
+def roofline(res, peak_gbs, peak_kind):
+    S, nb = res["stream_bytes"], res["input_bytes"]
+    traffic = traffic_summary().get(res["workload"], {})
+    out = {}
+    for k in ("compress", "decompress"):
+        alg = nb + S
+        ms = res[f"{k}_ms"]
+        ach = alg / (ms / 1e3) / 1e9
+        t = traffic.get(k)
+        out[k] = {"gbs_input": nb / (ms / 1e3) / 1e9, "ms": ms, "bound": "hbm", "achieved": ach, "peak": peak_gbs,
+                  "unit": "GB/s", "frac": ach / peak_gbs, "frac_of_8000": ach / 8000.0,
+                  "traffic": (t * 1.0) if t is not None else None, "algorithmic_bytes": alg,
+                  "peak_kind": peak_kind}
+    return out
+
+
+def run_batched(device, count=4096, steps=5, seed=3):
+    """Batched form: `count` f32 arrays, element counts log-uniform in [2^8, 2^24];
+    85% N(0, 0.02) weight-like values (fixed mode), 10% the sinusoid field (plain),
+    5% all zeros (fixed); every array rel eb 1e-3.  One autotuned, graph-captured
+    persistent launch (device value ranges + codec) against per-array calls, with
+    byte-identical output per array."""
+    import numpy as np
+    import torch
+    from cuszp_b200 import batch, codec, datagen
+    from cuszp_b200.pycuSZp import cuSZp
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(2 ** 8), np.log(2 ** 24), count)).astype(np.int64)
+    kinds = rng.choice(3, size=count, p=[0.85, 0.10, 0.05])
+    xs, modes = [], []
+    sin = datagen.sinusoid_field(1 << 24, seed=0, device=device)
+    for i in range(count):
+        n = int(sizes[i])
+        if kinds[i] == 0:
+            xs.append(datagen.weight_like(n, seed=seed * 100003 + i, device=device))
+            modes.append("fixed")
+        elif kinds[i] == 1:
+            xs.append(sin[:n].clone())
+            modes.append("plain")
+        else:
+            xs.append(torch.zeros(n, device=device))
+            modes.append("fixed")
+    total = int(sum(x.numel() for x in xs)) * 4
+    plan = batch.compress_plan(xs, [1e-3] * count, modes, rel=[True] * count)
+    cfg = plan.tune(reps=2)
+    plan.capture()
+    torch.cuda.synchronize()
+    plan.replay()
+    torch.cuda.synchronize()
+    plan.check()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        plan.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    b_ms = e0.elapsed_time(e1) / steps
+    bsizes = plan.sizes.cpu().tolist()
+    ebs = plan.error_bounds()
+
+    # plain: per-array reference-compatible calls (device range -> eb, then cuSZp_compress)
+    api = cuSZp()
+    outs = [torch.empty(max(16, codec.max_compressed_size(codec.Layout.of(x), x.dtype, m)), dtype=torch.uint8,
+                        device=device) for x, m in zip(xs, modes)]
+    identical = True
+    psz = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, x in enumerate(xs):
+        eb = codec.rel_error_bound(x, 1e-3)
+        psz.append(api.compress(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(outs[i].data_ptr()), x.numel(), eb,
+                                dim=1, dims=(0, 0, 0), data_type=0, mode=codec.MODES[modes[i]]))
+    torch.cuda.synchronize()
+    p_s = time.perf_counter() - t0
+    for i in range(count):
+        if psz[i] != bsizes[i] or not torch.equal(outs[i][: psz[i]], plan.outputs[i][: bsizes[i]]):
+            identical = False
+            break
+    # plain, asynchronous: per-array launches on one stream, bounds precomputed
+    ws = codec.Workspace(device)
+    sz = torch.zeros(1, dtype=torch.int64, device=device)
+    for _ in range(2):
+        e0.record()
+        for i, x in enumerate(xs):
+            codec.compress_into(x, outs[i], ebs[i], modes[i], size_out=sz, workspace=ws)
+        e1.record()
+        torch.cuda.synchronize()
+    a_ms = e0.elapsed_time(e1)
+    plan.close()
+    del xs, outs
+    return {"arrays": count, "input_bytes": total, "batched_ms": b_ms, "batched_gbs": total / (b_ms / 1e3) / 1e9,
+            "plain_sync_ms": p_s * 1e3, "plain_sync_gbs": total / p_s / 1e9,
+            "plain_async_ms": a_ms, "plain_async_gbs": total / (a_ms / 1e3) / 1e9,
+            "speedup_vs_plain_sync": p_s * 1e3 / b_ms, "speedup_vs_plain_async": a_ms / b_ms,
+            "byte_identical_per_array": identical, "autotuned": cfg,
+            "batched_includes": "device value ranges (rel eb) + codec, one graph replay",
+            "plain_sync_includes": "per array: device value range + cuSZp_compress (host sync)",
+            "plain_async_includes": "per array: cuSZp_compress_async on one stream, eb precomputed"}
+
+
+def run_serving(device, rates=(1000.0, 5000.0, 20000.0, 50000.0), count=1500, seed=4):
+    """Serving form: open-loop Poisson arrivals, 70% compress / 30% decompress, 4 KiB-256 MiB
+    log-uniform, 80% f32, modes uniform, 1D/2D/3D, abs eb log-uniform [1e-5, 1e-2], 64 GiB
+    budget; continuous batching against one-request-at-a-time calls."""
+    import torch
+    from cuszp_b200 import serve
+    pools = serve.make_pools(device)
+    out = {}
+    for rate in rates:
+        reqs = serve.make_requests(count, rate, pools, seed=seed)
+        srv = serve.Server(device, budget_bytes=64 << 30)
+        b = srv.run(reqs, open_loop=True)
+        batched = [r.result for r in reqs]
+        serve.reset(reqs)
+        seq = serve.serve_sequential(reqs, open_loop=True)
+        same = all(torch.equal(a.reshape(-1).view(torch.uint8), r.result.reshape(-1).view(torch.uint8))
+                   for a, r in zip(batched, reqs))
+        out[f"{int(rate)}"] = {"batched": b, "one_at_a_time": seq, "identical_results": same}
+        del reqs, batched
+        torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-also", action="store_true", help="skip the extra workloads")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and serving forms")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        return reference_arm(args)
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+        pg = dist
+    stream = torch.cuda.Stream(device)
+    if pg:
+        pg.barrier()
+    res = run_workload(args.workload, args.steps, args.warmup, device, stream, rank, measure_e2e=not args.no_e2e)
+    total_s = res["total_ms"] / 1e3
+    e2e_ms = res["e2e"]["value"] if "e2e" in res else 0.0
+    if pg:
+        t = torch.tensor([total_s, -e2e_ms], dtype=torch.float64, device=device)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_s = float(t[0].item())
+        e2e_min = -float(t[1].item())
+        pg.barrier()
+        pg.destroy_process_group()
+    else:
+        e2e_min = e2e_ms
+    if rank != 0:
+        return
+    peak, kind = peaks()
+    rl = roofline(res, peak, kind)
+    dominant = "compress" if res["compress_ms"] >= res["decompress_ms"] else "decompress"
+    value = world * res["input_bytes"] * args.steps / total_s / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": res["dtype"], "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "desc": res["desc"], "n": res["n"], "dims": res["dims"],
+                   "mode": res["mode"], "dim": res["dim"], "eb": res["eb"], "step": "compress + decompress",
+                   "l2": "inputs (512 MiB) larger than L2 (126 MB); no flush needed",
+                   "parallelism": f"replicas x{world}"},
+        "compress": rl["compress"], "decompress": rl["decompress"],
+        "roofline": {k: rl[dominant][k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic")},
+        "roofline_kernel": dominant, "cr": res["cr"], "stream_bytes": res["stream_bytes"],
+        "error_check": {"over_eb": res["over_eb"], "over_1.1eb": res["over_1.1eb"],
+                        "max_err_over_eb": res["max_err_over_eb"]},
+        "e2e": dict(res["e2e"], value=world * e2e_min) if "e2e" in res else None,
+        "gpu_launches": res["launches"], "clocks": res["clocks"],
+    }
+    if not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args.workload, device)
+    if not args.no_also:
+        also = {}
+        for name in ALSO:
+            r = run_workload(name, max(5, args.steps // 2), args.warmup, device, stream, 0, measure_e2e=False)
+            rr = roofline(r, peak, kind)
+            also[name] = {"compress_gbs": rr["compress"]["gbs_input"], "decompress_gbs": rr["decompress"]["gbs_input"],
+                          "compress_frac": rr["compress"]["frac"], "decompress_frac": rr["decompress"]["frac"],
+                          "compress_frac_of_8000": rr["compress"]["frac_of_8000"],
+                          "decompress_frac_of_8000": rr["decompress"]["frac_of_8000"],
+                          "compress_ms": r["compress_ms"], "decompress_ms": r["decompress_ms"], "cr": r["cr"],
+                          "over_1.1eb": r["over_1.1eb"], "launches": r["launches"]}
+            line["gpu_launches"] += r["launches"]
+        line["also"] = also
+    if not args.no_forms and world == 1:
+        try:
+            line["batched"] = run_batched(device)
+        except Exception as e:
+            line["batched"] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+        try:
+            line["serving"] = run_serving(device)
+        except Exception as e:
+            line["serving"] = {"error": f"{type(e).__name__}: {e}"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- reference arm
+
+def reference_arm(args):
+    """CPU oracle on the host cores (the reference has no CPU path), plus the
+    reference's CUDA build (sm_100) timed on the same GPU through its C API."""
+    import torch
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    base = cpu_baseline(args.workload, device)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": WORKLOADS[args.workload][1], "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload][0], "step": "compress + decompress"},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    try:
+        line["reference_cuda_build"] = reference_cuda(args.workload, args.steps, args.warmup, device)
+    except Exception as e:  # the CPU arm above is the reference arm; the GPU build is extra
+        line["reference_cuda_build"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    print(json.dumps(line), flush=True)
+
+
+def reference_cuda(name, steps, warmup, device):
+    """The reference library compiled for sm_100 from its own sources (oracle/_ref),
+    called through cuSZp_compress/cuSZp_decompress on device buffers, timed with
+    CUDA events around each call (includes its per-call scratch malloc/free and
+    blocking size read-back, as its CLI's timing does)."""
+    import torch
+    from cuszp_b200 import codec
+    path = os.path.join(ROOT, "oracle", "_ref", "libcuszp_ref.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libcuszp_ref.so not built"}
+    lib = ctypes.CDLL(path)
+    from cuszp_b200.pycuSZp import Uint3
+    lib.cuSZp_compress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                   ctypes.POINTER(ctypes.c_size_t), ctypes.c_float, ctypes.c_int, Uint3,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.cuSZp_decompress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
+                                     ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    desc, dt, mode, dim, shape, ebk, ebv, gen = WORKLOADS[name]
+    x = make_input(name, device)
+    lay = codec.Layout.of(x, dim)
+    eb = codec.rel_error_bound(x, ebv) if ebk == "rel" else ebv
+    cap = codec.max_compressed_size(lay, x.dtype, mode)
+    d_c = torch.zeros(cap, dtype=torch.uint8, device=device)
+    d_o = torch.zeros_like(x)
+    t, m = codec.TYPES[x.dtype], codec.MODES[mode]
+    cs = ctypes.c_size_t(0)
+    d3 = Uint3(*lay.dims)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def comp():
+        lib.cuSZp_compress(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(d_c.data_ptr()), lay.n, ctypes.byref(cs),
+                           ctypes.c_float(eb), dim, d3, t, m, s)
+
+    def decomp():
+        lib.cuSZp_decompress(ctypes.c_void_p(d_o.data_ptr()), ctypes.c_void_p(d_c.data_ptr()), lay.n, cs.value,
+                             ctypes.c_float(eb), dim, d3, t, m, s)
+
+    for _ in range(warmup):
+        comp()
+        decomp()
+    torch.cuda.synchronize()
+    cms, dms = [], []
+    for _ in range(steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        comp()
+        e[1].record()
+        decomp()
+        e[2].record()
+        torch.cuda.synchronize()
+        cms.append(e[0].elapsed_time(e[1]))
+        dms.append(e[1].elapsed_time(e[2]))
+    nb = x.numel() * x.element_size()
+    c, d = statistics.mean(cms), statistics.mean(dms)
+    return {"compress_gbs": nb / (c / 1e3) / 1e9, "decompress_gbs": nb / (d / 1e3) / 1e9,
+            "round_trip_gbs": nb / ((c + d) / 1e3) / 1e9, "compress_ms": c, "decompress_ms": d,
+            "reported_cmpSize": cs.value, "build": "reference sources, nvcc -O3 sm_100 (oracle/Makefile ref)"}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,452 @@
+// batch.cu -- batched compression/decompression of many arrays in one persistent
+// launch, behind a plan object (include/cuSZp.h: cuSZp_batch_*):
+//   plan_create  -> device item table, tile map and value-range chunk map (once)
+//   plan_tune    -> autotuner: tile shape (warps x blocks per warp) and CTAs per SM
+//   plan_execute -> [value-range pass -> eb per array] -> one codec launch;
+//                   only kernel launches on the stream, so it can be captured in
+//                   a CUDA graph and replayed.
+// Per array the output is byte-identical to the single-array path: the tile body
+// is the same compress_tile / decompress_tile, with each array's own look-back chain.
+#include "../../include/cuSZp.h"
+#include "batch.cuh"
+#include "codec_kernels.cuh"
+#include "codec_launch.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace cuszp {
+
+// ------------------------------------------------------------------ maps and value ranges
+
+__global__ void fill_maps_kernel(const BatchItem* __restrict__ items, int n, uint32_t* __restrict__ tile_map,
+                                 uint32_t* __restrict__ chunk_map)
+{
+    for (int a = blockIdx.x; a < n; a += gridDim.x) {
+        const BatchItem& it = items[a];
+        for (uint64_t t = threadIdx.x; t < it.g.ntiles; t += blockDim.x) tile_map[it.tile_start + t] = (uint32_t)a;
+        if (chunk_map)
+            for (uint64_t c = threadIdx.x; c < it.nchunks; c += blockDim.x) chunk_map[it.chunk_start + c] = (uint32_t)a;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+range_partial_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ chunk_map,
+                     uint64_t total_chunks, double* __restrict__ partial)
+{
+    __shared__ double smx[8], smn[8];
+    for (uint64_t c = blockIdx.x; c < total_chunks; c += gridDim.x) {
+        const BatchItem& it = items[chunk_map[c]];
+        const T* in = static_cast<const T*>(it.in);
+        const uint64_t n = it.g.nbEle;
+        const uint64_t lo = (c - it.chunk_start) * kRangeChunk;
+        const uint64_t hi = min(n, lo + kRangeChunk);
+        T mx = -INFINITY, mn = INFINITY;   // NaN-skipping
+        for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            const T v = __ldcs(in + i);
+            mx = fmax(mx, v);
+            mn = fmin(mn, v);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+            mn = fmin(mn, __shfl_xor_sync(FULL, mn, o));
+        }
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) { smx[warp] = (double)mx; smn[warp] = (double)mn; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = smx[0], b = smn[0];
+            for (int w = 1; w < (int)(blockDim.x / 32); w++) { a = fmax(a, smx[w]); b = fmin(b, smn[w]); }
+            partial[2 * c] = b;
+            partial[2 * c + 1] = a;
+        }
+        __syncthreads();
+    }
+}
+
+// eb = rel * (max - min) with the reference CLI's float arithmetic
+// (examples/cuSZp.cpp:186 f32, :209 f64); NaN-first arrays give NaN.
+template <typename T>
+__global__ void range_finalize_kernel(BatchItem* __restrict__ items, int n, const double* __restrict__ partial)
+{
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        BatchItem& it = items[a];
+        if (it.rel < 0.0f || it.nchunks == 0) continue;   // absolute bound given
+        double mn = INFINITY, mx = -INFINITY;
+        for (uint64_t c = it.chunk_start; c < it.chunk_start + it.nchunks; c++) {
+            mn = fmin(mn, partial[2 * c]);
+            mx = fmax(mx, partial[2 * c + 1]);
+        }
+        const T first = static_cast<const T*>(it.in)[0];
+        if (first != first) { mn = (double)first; mx = (double)first; }
+        if (sizeof(T) == 4) it.eb = it.rel * ((float)mx - (float)mn);
+        else it.eb = it.rel * (float)(mx - mn);
+    }
+}
+
+// ------------------------------------------------------------------ batched codec
+
+template <typename T> __device__ __forceinline__ T recip_of(float eb);
+template <> __device__ __forceinline__ float recip_of<float>(float eb) { return __fdiv_rn(0.5f, eb); }
+template <> __device__ __forceinline__ double recip_of<double>(float eb) { return __ddiv_rn(0.5, (double)eb); }
+
+template <typename T, int DIM, typename Tl>
+__global__ void __launch_bounds__(Tl::THREADS)
+compress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
+                      uint64_t total_tiles, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status,
+                      unsigned long long* __restrict__ sizes)
+{
+    __shared__ uint32_t s_warp[Tl::WARPS];
+    __shared__ uint64_t s_base;
+    __shared__ int64_t s_tile;
+    __shared__ uint32_t s_item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
+            if ((uint64_t)s_tile < total_tiles) s_item = tile_map[s_tile];
+        }
+        __syncthreads();
+        const int64_t tile = s_tile;
+        if ((uint64_t)tile >= total_tiles) break;
+        const uint32_t a = s_item;
+        const BatchItem& it = items[a];
+        const Geom g = it.g;
+        const int64_t local = tile - (int64_t)it.tile_start;
+        unsigned long long* st = status + it.tile_start;
+        const T* in = static_cast<const T*>(it.in);
+        uint8_t* out = static_cast<uint8_t*>(it.out);
+        const T recip = recip_of<T>(it.eb);
+        switch (it.mode) {
+            case 0: compress_tile<T, DIM, 0, Tl>(in, out, g, recip, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
+            case 1: compress_tile<T, DIM, 1, Tl>(in, out, g, recip, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
+            default: compress_tile<T, DIM, 2, Tl>(in, out, g, recip, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
+        }
+    }
+    finish_cta(hdr, status, total_tiles);
+}
+
+template <typename T, int DIM, typename Tl>
+__global__ void __launch_bounds__(Tl::THREADS)
+decompress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
+                        uint64_t total_tiles, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status,
+                        unsigned long long* __restrict__ sizes)
+{
+    __shared__ uint32_t s_warp[Tl::WARPS];
+    __shared__ uint64_t s_base;
+    __shared__ int64_t s_tile;
+    __shared__ uint32_t s_item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
+            if ((uint64_t)s_tile < total_tiles) s_item = tile_map[s_tile];
+        }
+        __syncthreads();
+        const int64_t tile = s_tile;
+        if ((uint64_t)tile >= total_tiles) break;
+        const uint32_t a = s_item;
+        const BatchItem& it = items[a];
+        const Geom g = it.g;
+        const int64_t local = tile - (int64_t)it.tile_start;
+        unsigned long long* st = status + it.tile_start;
+        const uint8_t* in = static_cast<const uint8_t*>(it.in);
+        T* out = static_cast<T*>(it.out);
+        const T eb = (T)it.eb;
+        switch (it.mode) {
+            case 0: decompress_tile<T, DIM, 0, Tl>(out, in, g, eb, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
+            case 1: decompress_tile<T, DIM, 1, Tl>(out, in, g, eb, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
+            default: decompress_tile<T, DIM, 2, Tl>(out, in, g, eb, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
+        }
+    }
+    finish_cta(hdr, status, total_tiles);
+}
+
+// ------------------------------------------------------------------ tile-shape variants
+
+struct Variant {
+    int warps, bpw1, bpwn;   // warps per CTA; data blocks per warp in 1D and in 2D/3D
+    const void* (*kernel)(int type, int dim, bool comp);
+};
+
+template <int DIM, int WARPS, int BPW>
+static const void* kernel_for_variant(int type, bool comp)
+{
+    using Tl = Tiling<DIM, WARPS, BPW>;
+    if (type == 0) return comp ? (const void*)compress_batch_kernel<float, DIM, Tl> : (const void*)decompress_batch_kernel<float, DIM, Tl>;
+    return comp ? (const void*)compress_batch_kernel<double, DIM, Tl> : (const void*)decompress_batch_kernel<double, DIM, Tl>;
+}
+
+template <int WARPS, int BPW1D, int BPWND>
+static const void* kv(int type, int dim, bool comp)
+{
+    if (dim == 1) return kernel_for_variant<1, WARPS, BPW1D>(type, comp);
+    if (dim == 2) return kernel_for_variant<2, WARPS, BPWND>(type, comp);
+    return kernel_for_variant<3, WARPS, BPWND>(type, comp);
+}
+
+// (warps per CTA, blocks per warp in 1D, blocks per warp in 2D/3D)
+static const Variant kVariants[] = {
+    {8, 16, 8, kv<8, 16, 8>},
+    {4, 16, 8, kv<4, 16, 8>},
+    {8, 8, 4, kv<8, 8, 4>},
+    {16, 8, 4, kv<16, 8, 4>},
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+}  // namespace cuszp
+
+using namespace cuszp;
+
+struct cuszp_batch_plan {
+    int count = 0;
+    int dim = 1, type = 0;
+    bool compress = true;
+    bool any_rel = false;
+    int variant = 0;
+    int ctas_per_sm = 0;       // 0: occupancy limit
+    int sms = 148;
+    std::vector<cuszp_batch_item_t> host_items;
+    std::vector<BatchItem> items;
+    BatchItem* d_items = nullptr;
+    void* d_ws = nullptr;      // header + status + tile map + chunk map + partials
+    size_t ws_bytes = 0;
+    uint64_t total_tiles = 0, total_chunks = 0;
+    size_t status_off = 0, map_off = 0, cmap_off = 0, part_off = 0;
+};
+
+// (Re)builds the device item table, workspace and maps for a tile shape.  All
+// device work is stream-ordered on `s`; nothing here synchronizes the device.
+static int plan_layout(cuszp_batch_plan* p, int variant, cudaStream_t s)
+{
+    const Variant& v = kVariants[variant];
+    const int tb = v.warps * (p->dim == 1 ? v.bpw1 : v.bpwn);
+    uint64_t tiles = 0, chunks = 0;
+    for (int a = 0; a < p->count; a++) {
+        const cuszp_batch_item_t& h = p->host_items[a];
+        Problem pr;
+        int st = make_problem(pr, p->type, h.mode, p->dim, h.nbEle, h.dims.x, h.dims.y, h.dims.z);
+        if (st) return st;
+        Geom g = pr.g;
+        if (p->dim == 1) g.ntiles = g.rate_bytes / (uint64_t)tb;
+        else g.ntiles = (g.nblocks + tb - 1) / tb;
+        BatchItem& it = p->items[a];
+        std::memset(&it, 0, sizeof(it));
+        it.in = h.d_in;
+        it.out = h.d_out;
+        it.g = g;
+        it.tile_start = tiles;
+        it.mode = h.mode;
+        it.eb = h.rel ? 0.0f : h.errorBound;
+        it.rel = h.rel ? h.errorBound : -1.0f;
+        it.chunk_start = chunks;
+        it.nchunks = (h.rel && p->compress) ? (g.nbEle + kRangeChunk - 1) / kRangeChunk : 0;
+        tiles += g.ntiles;
+        chunks += it.nchunks;
+    }
+    p->total_tiles = tiles;
+    p->total_chunks = chunks;
+    p->status_off = sizeof(WsHeader);
+    p->map_off = p->status_off + 8 * (tiles ? tiles : 1);
+    p->cmap_off = (p->map_off + 4 * (tiles ? tiles : 1) + 15) / 16 * 16;
+    p->part_off = (p->cmap_off + 4 * (chunks ? chunks : 1) + 15) / 16 * 16;
+    const size_t need = p->part_off + 16 * (chunks ? chunks : 1);
+    if (need > p->ws_bytes) {
+        if (p->d_ws) cudaFreeAsync(p->d_ws, s);
+        p->d_ws = nullptr;
+        if (cudaMallocAsync(&p->d_ws, need, s) != cudaSuccess) return E_CUDA;
+        p->ws_bytes = need;
+    }
+    if (cudaMemsetAsync(p->d_ws, 0, p->ws_bytes, s) != cudaSuccess) return E_CUDA;
+    // pageable source: staged before the call returns, so `items` may change afterwards
+    if (p->count && cudaMemcpyAsync(p->d_items, p->items.data(), sizeof(BatchItem) * p->count,
+                                    cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return E_CUDA;
+    char* ws = static_cast<char*>(p->d_ws);
+    if (p->count)
+        fill_maps_kernel<<<std::min(p->count, 4096), 256, 0, s>>>(p->d_items, p->count, (uint32_t*)(ws + p->map_off),
+                                                                  chunks ? (uint32_t*)(ws + p->cmap_off) : nullptr);
+    if (cudaGetLastError() != cudaSuccess) return E_CUDA;
+    p->variant = variant;
+    return OK;
+}
+
+static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStream_t s)
+{
+    char* ws = static_cast<char*>(p->d_ws);
+    if (p->compress && p->total_chunks) {
+        const unsigned grid = (unsigned)std::min<uint64_t>(p->total_chunks, (uint64_t)p->sms * 8);
+        double* part = (double*)(ws + p->part_off);
+        const uint32_t* cmap = (const uint32_t*)(ws + p->cmap_off);
+        if (p->type == 0) {
+            range_partial_kernel<float><<<grid, 256, 0, s>>>(p->d_items, cmap, p->total_chunks, part);
+            range_finalize_kernel<float><<<(p->count + 127) / 128, 128, 0, s>>>(p->d_items, p->count, part);
+        } else {
+            range_partial_kernel<double><<<grid, 256, 0, s>>>(p->d_items, cmap, p->total_chunks, part);
+            range_finalize_kernel<double><<<(p->count + 127) / 128, 128, 0, s>>>(p->d_items, p->count, part);
+        }
+    }
+    if (p->total_tiles == 0) return cudaGetLastError() == cudaSuccess ? OK : E_CUDA;
+    const Variant& v = kVariants[p->variant];
+    const void* fn = v.kernel(p->type, p->dim, p->compress);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.warps * 32, 0);
+    if (occ < 1) occ = 1;
+    const int per_sm = p->ctas_per_sm > 0 ? std::min(p->ctas_per_sm, occ) : occ;
+    const uint64_t want = (uint64_t)p->sms * per_sm;
+    const unsigned grid = (unsigned)std::min<uint64_t>(want, p->total_tiles);
+    const BatchItem* items = p->d_items;
+    const uint32_t* map = (const uint32_t*)(ws + p->map_off);
+    uint64_t total = p->total_tiles;
+    WsHeader* hdr = (WsHeader*)ws;
+    unsigned long long* status = (unsigned long long*)(ws + p->status_off);
+    void* args[] = {(void*)&items, (void*)&map, (void*)&total, (void*)&hdr, (void*)&status, (void*)&d_sizes};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(v.warps * 32), args, 0, s) == cudaSuccess ? OK : E_CUDA;
+}
+
+extern "C" int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
+                                             cuszp_dim_t dim, cuszp_type_t type, int compress, cudaStream_t stream)
+{
+    if (!plan || count < 0 || (count && !items)) return E_ARG;
+    if (type != CUSZP_TYPE_FLOAT && type != CUSZP_TYPE_DOUBLE) return E_ARG;
+    if (dim < CUSZP_DIM_1D || dim > CUSZP_DIM_3D) return E_ARG;
+    auto* p = new cuszp_batch_plan;
+    p->count = count;
+    p->dim = dim;
+    p->type = type;
+    p->compress = compress != 0;
+    p->host_items.assign(items, items + count);
+    p->items.resize(count);
+    for (int a = 0; a < count; a++) {
+        const cuszp_batch_item_t& h = items[a];
+        if (h.mode < CUSZP_MODE_FIXED || h.mode > CUSZP_MODE_OUTLIER) { delete p; return E_ARG; }
+        if (h.nbEle && (!h.d_in || !h.d_out)) { delete p; return E_ARG; }
+        if (h.rel) p->any_rel = true;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaMallocAsync((void**)&p->d_items, sizeof(BatchItem) * (count ? count : 1), stream) != cudaSuccess) {
+        delete p;
+        return E_CUDA;
+    }
+    const int st = plan_layout(p, 0, stream);
+    if (st) {
+        cudaFreeAsync(p->d_items, stream);
+        if (p->d_ws) cudaFreeAsync(p->d_ws, stream);
+        delete p;
+        return st;
+    }
+    *plan = p;
+    return OK;
+}
+
+extern "C" int cuSZp_batch_plan_create(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
+                                       cuszp_dim_t dim, cuszp_type_t type, int compress)
+{
+    const int st = cuSZp_batch_plan_create_async(plan, count, items, dim, type, compress, 0);
+    if (st) return st;
+    return cudaStreamSynchronize(0) == cudaSuccess ? OK : E_CUDA;
+}
+
+extern "C" int cuSZp_batch_plan_execute(cuszp_batch_plan_t p, unsigned long long* d_sizes, cudaStream_t stream)
+{
+    if (!p || (p->count && !d_sizes)) return E_ARG;
+    return plan_launch(p, d_sizes, stream);
+}
+
+extern "C" int cuSZp_batch_plan_check(cuszp_batch_plan_t p, cudaStream_t stream)
+{
+    if (!p) return E_ARG;
+    return cuSZp_workspace_check(p->d_ws, p->ws_bytes, stream);
+}
+
+extern "C" int cuSZp_batch_plan_config(cuszp_batch_plan_t p, int* warps, int* blocks_per_warp, int* ctas_per_sm)
+{
+    if (!p) return E_ARG;
+    if (warps) *warps = kVariants[p->variant].warps;
+    if (blocks_per_warp) *blocks_per_warp = p->dim == 1 ? kVariants[p->variant].bpw1 : kVariants[p->variant].bpwn;
+    if (ctas_per_sm) *ctas_per_sm = p->ctas_per_sm;
+    return OK;
+}
+
+// Autotuner: times every tile shape x CTAs-per-SM candidate on this plan's own
+// arrays (CUDA events on `stream`, best of `reps`) and keeps the fastest.
+extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d_sizes, int reps, cudaStream_t stream)
+{
+    if (!p || (p->count && !d_sizes)) return E_ARG;
+    if (reps < 1) reps = 1;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int best_v = 0, best_c = 0;
+    for (int v = 0; v < kNumVariants; v++) {
+        int st = plan_layout(p, v, stream);
+        if (st) return st;
+        const void* fn = kVariants[v].kernel(p->type, p->dim, p->compress);
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].warps * 32, 0);
+        for (int c = 1; c <= std::max(1, occ); c++) {
+            p->ctas_per_sm = c;
+            plan_launch(p, d_sizes, stream);   // warm
+            float t_best = 1e30f;
+            for (int r = 0; r < reps; r++) {
+                cudaEventRecord(e0, stream);
+                plan_launch(p, d_sizes, stream);
+                cudaEventRecord(e1, stream);
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                t_best = std::min(t_best, ms);
+            }
+            if (t_best < best) { best = t_best; best_v = v; best_c = c; }
+        }
+        if (cuSZp_workspace_check(p->d_ws, p->ws_bytes, stream)) return E_TIMEOUT;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int st = plan_layout(p, best_v, stream);
+    p->ctas_per_sm = best_c;
+    if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = E_CUDA;
+    return st;
+}
+
+extern "C" int cuSZp_batch_plan_set_config(cuszp_batch_plan_t p, int variant, int ctas_per_sm)
+{
+    if (!p || variant < 0 || variant >= kNumVariants) return E_ARG;
+    const int st = plan_layout(p, variant, 0);
+    p->ctas_per_sm = ctas_per_sm;
+    if (st) return st;
+    return cudaStreamSynchronize(0) == cudaSuccess ? OK : E_CUDA;
+}
+
+extern "C" void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t p, cudaStream_t stream)
+{
+    if (!p) return;
+    if (p->d_items) cudaFreeAsync(p->d_items, stream);
+    if (p->d_ws) cudaFreeAsync(p->d_ws, stream);
+    delete p;
+}
+
+extern "C" void cuSZp_batch_plan_destroy(cuszp_batch_plan_t p)
+{
+    if (!p) return;
+    cudaDeviceSynchronize();
+    cuSZp_batch_plan_destroy_async(p, 0);
+    cudaStreamSynchronize(0);
+}
+
+extern "C" int cuSZp_batch_plan_eb(cuszp_batch_plan_t p, float* errorBounds, cudaStream_t stream)
+{
+    if (!p || !errorBounds) return E_ARG;
+    std::vector<BatchItem> tmp(p->count);
+    if (p->count) {
+        if (cudaMemcpyAsync(tmp.data(), p->d_items, sizeof(BatchItem) * p->count, cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+            return E_CUDA;
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return E_CUDA;
+    }
+    for (int a = 0; a < p->count; a++) errorBounds[a] = tmp[a].eb;
+    return OK;
+}

@@ -21,7 +21,7 @@
 namespace cuszp {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int kWarps = 8;
+constexpr int kWarps = 8;                 // default warps per CTA of the single-array kernels
 constexpr int kThreads = kWarps * 32;
 
 enum Mode : int { MODE_FIXED = 0, MODE_PLAIN = 1, MODE_OUTLIER = 2 };
@@ -219,34 +219,36 @@ __device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* st
 
 // CTA-wide tile prefix: warp totals -> tile aggregate -> publish -> look-back.
 // Returns (through shared memory) the tile's exclusive byte offset and each warp's
-// offset inside the tile.  Called by all threads.
+// offset inside the tile; the last tile of an array stores the stream length S in
+// *total_out.  Called by all threads.
+template <int WARPS>
 __device__ __forceinline__ void tile_scan(uint32_t warp_total, int64_t tile, uint64_t ntiles,
-                                          unsigned long long* status, WsHeader* hdr, uint64_t rate_bytes,
-                                          uint32_t* s_warp, uint64_t* s_base)
+                                          unsigned long long* status, uint32_t* err, unsigned long long* total_out,
+                                          uint64_t rate_bytes, uint32_t* s_warp, uint64_t* s_base)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) s_warp[warp] = warp_total;
     __syncthreads();
     if (warp == 0) {
-        uint32_t v = lane < kWarps ? s_warp[lane] : 0u;
+        uint32_t v = lane < WARPS ? s_warp[lane] : 0u;
         uint32_t incl = v;
 #pragma unroll
-        for (int o = 1; o < kWarps; o <<= 1) {
+        for (int o = 1; o < WARPS; o <<= 1) {
             uint32_t t = __shfl_up_sync(FULL, incl, o);
             if (lane >= o) incl += t;
         }
-        const uint64_t agg = __shfl_sync(FULL, incl, kWarps - 1);
+        const uint64_t agg = __shfl_sync(FULL, incl, WARPS - 1);
         __syncwarp();
-        if (lane < kWarps) s_warp[lane] = incl - v;
+        if (lane < WARPS) s_warp[lane] = incl - v;
         if (lane == 0) st_release(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
         uint64_t excl = 0;
         if (tile > 0) {
-            excl = lookback(status, tile, &hdr->err, lane);
+            excl = lookback(status, tile, err, lane);
             if (lane == 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
         }
         if (lane == 0) {
             *s_base = excl;
-            if ((uint64_t)tile == ntiles - 1) hdr->total = rate_bytes + excl + agg;
+            if ((uint64_t)tile == ntiles - 1) *total_out = rate_bytes + excl + agg;
         }
     }
     __syncthreads();

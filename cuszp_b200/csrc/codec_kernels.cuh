@@ -17,10 +17,17 @@
 
 namespace cuszp {
 
-template <int DIM> struct Tiling {
-    static constexpr int BPW = DIM == 1 ? 16 : 8;   // data blocks per warp per tile
-    static constexpr int TB = kWarps * BPW;         // data blocks per tile
+// Tile shape: WARPS warps per CTA, BPW data blocks per warp (TB = WARPS*BPW per tile).
+// In 1D a tile count must divide the 1024-block rate-region granule, so TB is a
+// power of two <= 1024.
+template <int DIM, int WARPS_ = kWarps, int BPW_ = (DIM == 1 ? 16 : 8)> struct Tiling {
+    static constexpr int DIMS = DIM;
+    static constexpr int WARPS = WARPS_;
+    static constexpr int THREADS = 32 * WARPS_;
+    static constexpr int BPW = BPW_;                // data blocks per warp per tile
+    static constexpr int TB = WARPS_ * BPW_;        // data blocks per tile
     static constexpr int W = DIM == 1 ? 4 : 8;      // bytes per bit-plane
+    static_assert(BPW_ % 2 == 0 && BPW_ <= 32, "blocks per warp");
 };
 
 // --------------------------------------------------------------- byte stores / loads
@@ -170,24 +177,16 @@ __device__ __forceinline__ void lorenzo_inverse(int32_t& d0, int32_t& d1, int la
 
 // --------------------------------------------------------------- compress
 
-template <typename T, int DIM, int MODE>
-__global__ void __launch_bounds__(kThreads)
-compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T recip,
-                WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
+__device__ __forceinline__ void compress_tile(const T* __restrict__ in, uint8_t* __restrict__ cmp, const Geom& g,
+                                              T recip, int64_t tile, unsigned long long* __restrict__ status,
+                                              uint32_t* err, unsigned long long* total_out, uint32_t* s_warp,
+                                              uint64_t* s_base)
 {
-    using Tl = Tiling<DIM>;
     constexpr int BPW = Tl::BPW;
     constexpr int W = Tl::W;
-    __shared__ uint32_t s_warp[kWarps];
-    __shared__ uint64_t s_base;
-    __shared__ int64_t s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
-        __syncthreads();
-        const int64_t tile = s_tile;
-        if ((uint64_t)tile >= g.ntiles) break;
+    {
         const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
 
         // ---- 1. load, quantize, predict
@@ -265,8 +264,8 @@ compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T r
         if (lane < BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)myrb;
 
         // ---- 2. tile offset
-        tile_scan(wtot, tile, g.ntiles, status, hdr, g.rate_bytes, s_warp, &s_base);
-        uint8_t* const pbase = cmp + g.rate_bytes + s_base + s_warp[warp];
+        tile_scan<Tl::WARPS>(wtot, tile, g.ntiles, status, err, total_out, g.rate_bytes, s_warp, s_base);
+        uint8_t* const pbase = cmp + g.rate_bytes + *s_base + s_warp[warp];
 
         // ---- 3. sign maps and bit-planes
         if constexpr (DIM == 1) {
@@ -348,28 +347,37 @@ compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T r
             }
         }
     }
-    finish_cta(hdr, status, g.ntiles);
 }
-
-// --------------------------------------------------------------- decompress
 
 template <typename T, int DIM, int MODE>
 __global__ void __launch_bounds__(kThreads)
-decompress_kernel(T* __restrict__ out, const uint8_t* __restrict__ cmp, Geom g, T eb,
-                  WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T recip,
+                WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
 {
-    using Tl = Tiling<DIM>;
-    constexpr int BPW = Tl::BPW;
     __shared__ uint32_t s_warp[kWarps];
     __shared__ uint64_t s_base;
     __shared__ int64_t s_tile;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
         __syncthreads();
         const int64_t tile = s_tile;
         if ((uint64_t)tile >= g.ntiles) break;
+        compress_tile<T, DIM, MODE>(in, cmp, g, recip, tile, status, &hdr->err, &hdr->total, s_warp, &s_base);
+    }
+    finish_cta(hdr, status, g.ntiles);
+}
+
+// --------------------------------------------------------------- decompress
+
+template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
+__device__ __forceinline__ void decompress_tile(T* __restrict__ out, const uint8_t* __restrict__ cmp, const Geom& g,
+                                                T eb, int64_t tile, unsigned long long* __restrict__ status,
+                                                uint32_t* err, unsigned long long* total_out, uint32_t* s_warp,
+                                                uint64_t* s_base)
+{
+    constexpr int BPW = Tl::BPW;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    {
         const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
 
         // ---- rate bytes -> payload sizes -> warp-local offsets
@@ -385,8 +393,8 @@ decompress_kernel(T* __restrict__ out, const uint8_t* __restrict__ cmp, Geom g, 
         const uint32_t myoff = incl - sz;
         const uint32_t wtot = __shfl_sync(FULL, incl, 31);
 
-        tile_scan(wtot, tile, g.ntiles, status, hdr, g.rate_bytes, s_warp, &s_base);
-        const uint8_t* const pbase = cmp + g.rate_bytes + s_base + s_warp[warp];
+        tile_scan<Tl::WARPS>(wtot, tile, g.ntiles, status, err, total_out, g.rate_bytes, s_warp, s_base);
+        const uint8_t* const pbase = cmp + g.rate_bytes + *s_base + s_warp[warp];
 
         if constexpr (DIM == 1) {
             // ---- load phase: plane words and sign words of all blocks
@@ -530,6 +538,23 @@ decompress_kernel(T* __restrict__ out, const uint8_t* __restrict__ cmp, Geom g, 
                 if (ok1) st_stream(out + i1, dequant(d1, eb));
             }
         }
+    }
+}
+
+template <typename T, int DIM, int MODE>
+__global__ void __launch_bounds__(kThreads)
+decompress_kernel(T* __restrict__ out, const uint8_t* __restrict__ cmp, Geom g, T eb,
+                  WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+{
+    __shared__ uint32_t s_warp[kWarps];
+    __shared__ uint64_t s_base;
+    __shared__ int64_t s_tile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
+        __syncthreads();
+        const int64_t tile = s_tile;
+        if ((uint64_t)tile >= g.ntiles) break;
+        decompress_tile<T, DIM, MODE>(out, cmp, g, eb, tile, status, &hdr->err, &hdr->total, s_warp, &s_base);
     }
     finish_cta(hdr, status, g.ntiles);
 }

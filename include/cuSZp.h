@@ -148,6 +148,48 @@ int cuSZp_rel_error_bound(const void* d_data, size_t nbEle, cuszp_type_t type, f
 int cuSZp_value_range(const void* d_data, size_t nbEle, cuszp_type_t type,
                       double* minValue, double* maxValue, cudaStream_t stream);
 
+/* ------------------------------------------------------------------ batches
+ * Many arrays compressed (or decompressed) by ONE persistent kernel launch that
+ * pulls tiles of all arrays from a device work queue; every array keeps its own
+ * look-back chain, so each array's stream is byte-identical to cuSZp_compress's.
+ * A plan owns the device item table and workspace; executing it only enqueues
+ * kernels, so it can be captured in a CUDA graph and replayed.  All arrays of a
+ * plan share dim and type; modes may differ per array. */
+
+typedef struct {
+    const void* d_in;      /* compress: data;   decompress: stream */
+    void* d_out;           /* compress: stream buffer (>= cuSZp_max_compressed_size); decompress: data */
+    size_t nbEle;
+    uint3 dims;
+    float errorBound;      /* absolute, or relative to the array's value range when rel != 0 */
+    int rel;               /* compress only: derive eb = errorBound*(max-min) on the device */
+    cuszp_mode_t mode;
+} cuszp_batch_item_t;
+
+typedef struct cuszp_batch_plan* cuszp_batch_plan_t;
+
+int cuSZp_batch_plan_create(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
+                            cuszp_dim_t dim, cuszp_type_t type, int compress);
+/* Same, with every device step (stream-ordered allocation, table upload, map build)
+ * enqueued on `stream` and no synchronization: for request loops that keep other
+ * work in flight. */
+int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
+                                  cuszp_dim_t dim, cuszp_type_t type, int compress, cudaStream_t stream);
+/* Enqueue the batch on `stream`; stream lengths go to d_sizes[count] (device u64). */
+int cuSZp_batch_plan_execute(cuszp_batch_plan_t plan, unsigned long long* d_sizes, cudaStream_t stream);
+/* Autotuner: time each tile shape (warps per CTA x blocks per warp) and CTAs per SM on
+ * this plan's arrays and keep the fastest (runs the batch several times). */
+int cuSZp_batch_plan_tune(cuszp_batch_plan_t plan, unsigned long long* d_sizes, int reps, cudaStream_t stream);
+int cuSZp_batch_plan_set_config(cuszp_batch_plan_t plan, int variant, int ctasPerSM);
+int cuSZp_batch_plan_config(cuszp_batch_plan_t plan, int* warps, int* blocksPerWarp, int* ctasPerSM);
+/* Absolute bounds the last execution used (derived on the device for rel items). */
+int cuSZp_batch_plan_eb(cuszp_batch_plan_t plan, float* errorBounds, cudaStream_t stream);
+/* Synchronize and report a timed-out device wait (CUSZP_ERROR_TIMEOUT). */
+int cuSZp_batch_plan_check(cuszp_batch_plan_t plan, cudaStream_t stream);
+void cuSZp_batch_plan_destroy(cuszp_batch_plan_t plan);
+/* Release a plan once the work already enqueued on `stream` is done (stream-ordered free). */
+void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t plan, cudaStream_t stream);
+
 /* Version string of this build. */
 const char* cuSZp_version(void);
 
