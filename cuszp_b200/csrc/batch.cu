@@ -6,13 +6,14 @@
 //                   only kernel launches on the stream, so it can be captured in
 //                   a CUDA graph and replayed.
 // Per array the output is byte-identical to the single-array path: the tile body
-// is the same compress_tile / decompress_tile, with each array's own look-back chain.
+// is the same pipelined compress/decompress phases, with each array's own look-back chain.
 #include "../../include/cuSZp.h"
 #include "batch.cuh"
 #include "codec_kernels.cuh"
 #include "codec_launch.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <vector>
 
@@ -93,72 +94,126 @@ template <typename T> __device__ __forceinline__ T recip_of(float eb);
 template <> __device__ __forceinline__ float recip_of<float>(float eb) { return __fdiv_rn(0.5f, eb); }
 template <> __device__ __forceinline__ double recip_of<double>(float eb) { return __ddiv_rn(0.5, (double)eb); }
 
+// Calls f(integral_constant<int, mode>) so per-array modes reach template code.
+template <typename F>
+__device__ __forceinline__ void with_mode(int mode, F&& f)
+{
+    switch (mode) {
+        case 0: f(std::integral_constant<int, 0>{}); break;
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        default: f(std::integral_constant<int, 2>{}); break;
+    }
+}
+
+// Thread 0 takes a ticket and looks up its array (tile_map) into slot `k`.
+template <int WARPS>
+__device__ __forceinline__ void take_ticket(TileShared<WARPS>& sh, uint32_t* s_item, int k, WsHeader* hdr,
+                                            const uint32_t* __restrict__ tile_map, uint64_t total_tiles)
+{
+    const int64_t t = (int64_t)atomicAdd(&hdr->ticket, 1u);
+    sh.ticket[k] = t;
+    s_item[k] = (uint64_t)t < total_tiles ? tile_map[t] : 0u;
+}
+
 template <typename T, int DIM, typename Tl>
-__global__ void __launch_bounds__(Tl::THREADS)
+__global__ void __launch_bounds__(Tl::THREADS, 512 / Tl::THREADS > 0 ? 512 / Tl::THREADS : 1)
 compress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
                       uint64_t total_tiles, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status,
                       unsigned long long* __restrict__ sizes)
 {
-    __shared__ uint32_t s_warp[Tl::WARPS];
-    __shared__ uint64_t s_base;
-    __shared__ int64_t s_tile;
-    __shared__ uint32_t s_item;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
-            if ((uint64_t)s_tile < total_tiles) s_item = tile_map[s_tile];
-        }
-        __syncthreads();
-        const int64_t tile = s_tile;
-        if ((uint64_t)tile >= total_tiles) break;
-        const uint32_t a = s_item;
+    __shared__ TileShared<Tl::WARPS> sh;
+    __shared__ uint32_t s_item[2];
+    if (threadIdx.x == 0) take_ticket<Tl::WARPS>(sh, s_item, 0, hdr, tile_map, total_tiles);
+    __syncthreads();
+    int64_t tile = sh.ticket[0];
+    uint32_t a = s_item[0];
+    CompressIn<T, DIM, Tl> L;
+    if ((uint64_t)tile < total_tiles) {
+        const BatchItem& it = items[a];
+        compress_load<T, DIM, Tl>(L, static_cast<const T*>(it.in), it.g, tile - (int64_t)it.tile_start);
+    }
+    for (int k = 1; (uint64_t)tile < total_tiles; k++) {
+        if (threadIdx.x == 0) take_ticket<Tl::WARPS>(sh, s_item, k & 1, hdr, tile_map, total_tiles);
         const BatchItem& it = items[a];
         const Geom g = it.g;
         const int64_t local = tile - (int64_t)it.tile_start;
-        unsigned long long* st = status + it.tile_start;
-        const T* in = static_cast<const T*>(it.in);
-        uint8_t* out = static_cast<uint8_t*>(it.out);
         const T recip = recip_of<T>(it.eb);
-        switch (it.mode) {
-            case 0: compress_tile<T, DIM, 0, Tl>(in, out, g, recip, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
-            case 1: compress_tile<T, DIM, 1, Tl>(in, out, g, recip, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
-            default: compress_tile<T, DIM, 2, Tl>(in, out, g, recip, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
-        }
+        uint8_t* out = static_cast<uint8_t*>(it.out);
+        unsigned long long* st = status + it.tile_start;
+        int64_t next = 0;
+        uint32_t an = 0;
+        auto load_next = [&](CompressIn<T, DIM, Tl>& Ln) {
+            next = sh.ticket[k & 1];
+            an = s_item[k & 1];
+            if ((uint64_t)next < total_tiles) {
+                const BatchItem& itn = items[an];
+                compress_load<T, DIM, Tl>(Ln, static_cast<const T*>(itn.in), itn.g, next - (int64_t)itn.tile_start);
+            }
+        };
+        with_mode(it.mode, [&](auto m) {
+            compress_step<T, DIM, decltype(m)::value, Tl>(L, g, recip, local, out, st, &hdr->err, sizes + a, sh,
+                                                          load_next);
+        });
+        tile = next;
+        a = an;
     }
     finish_cta(hdr, status, total_tiles);
 }
 
 template <typename T, int DIM, typename Tl>
-__global__ void __launch_bounds__(Tl::THREADS)
+__global__ void __launch_bounds__(Tl::THREADS, 512 / Tl::THREADS > 0 ? 512 / Tl::THREADS : 1)
 decompress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
                         uint64_t total_tiles, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status,
                         unsigned long long* __restrict__ sizes)
 {
-    __shared__ uint32_t s_warp[Tl::WARPS];
-    __shared__ uint64_t s_base;
-    __shared__ int64_t s_tile;
-    __shared__ uint32_t s_item;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
-            if ((uint64_t)s_tile < total_tiles) s_item = tile_map[s_tile];
-        }
+    __shared__ TileShared<Tl::WARPS> sh;
+    __shared__ uint32_t s_item[2];
+    if (threadIdx.x == 0) take_ticket<Tl::WARPS>(sh, s_item, 0, hdr, tile_map, total_tiles);
+    __syncthreads();
+    int64_t tile = sh.ticket[0];
+    uint32_t a = s_item[0];
+    int slot = 0;
+    DecompRates<Tl> R;
+    if ((uint64_t)tile < total_tiles) {
+        const BatchItem& it = items[a];
+        const int64_t local = tile - (int64_t)it.tile_start;
+        with_mode(it.mode, [&](auto m) {
+            decompress_rates<DIM, decltype(m)::value, Tl>(R, static_cast<const uint8_t*>(it.in), it.g, local);
+        });
+        post_aggregate<Tl::WARPS>(R.wtot, local, status + it.tile_start, sh.dwarp[0], &sh.dagg[0]);
+    }
+    for (int k = 1; (uint64_t)tile < total_tiles; k++) {
+        if (threadIdx.x == 0) take_ticket<Tl::WARPS>(sh, s_item, k & 1, hdr, tile_map, total_tiles);
         __syncthreads();
-        const int64_t tile = s_tile;
-        if ((uint64_t)tile >= total_tiles) break;
-        const uint32_t a = s_item;
+        const int64_t next = sh.ticket[k & 1];
+        const uint32_t an = s_item[k & 1];
+        DecompRates<Tl> Rn = R;
+        if ((uint64_t)next < total_tiles) {
+            const BatchItem& itn = items[an];
+            const int64_t ln = next - (int64_t)itn.tile_start;
+            with_mode(itn.mode, [&](auto m) {
+                decompress_rates<DIM, decltype(m)::value, Tl>(Rn, static_cast<const uint8_t*>(itn.in), itn.g, ln);
+            });
+            post_aggregate<Tl::WARPS>(Rn.wtot, ln, status + itn.tile_start, sh.dwarp[slot ^ 1], &sh.dagg[slot ^ 1]);
+        }
         const BatchItem& it = items[a];
         const Geom g = it.g;
         const int64_t local = tile - (int64_t)it.tile_start;
-        unsigned long long* st = status + it.tile_start;
-        const uint8_t* in = static_cast<const uint8_t*>(it.in);
-        T* out = static_cast<T*>(it.out);
+        const uint8_t* cmp = static_cast<const uint8_t*>(it.in);
+        const uint64_t excl = resolve_tile<Tl::WARPS>(local, g.ntiles, status + it.tile_start, &hdr->err, sizes + a,
+                                                      g.rate_bytes, sh.dagg[slot], sh.lb);
+        const uint8_t* pbase = cmp + g.rate_bytes + excl + sh.dwarp[slot][threadIdx.x >> 5];
         const T eb = (T)it.eb;
-        switch (it.mode) {
-            case 0: decompress_tile<T, DIM, 0, Tl>(out, in, g, eb, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
-            case 1: decompress_tile<T, DIM, 1, Tl>(out, in, g, eb, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
-            default: decompress_tile<T, DIM, 2, Tl>(out, in, g, eb, local, st, &hdr->err, sizes + a, s_warp, &s_base); break;
-        }
+        T* out = static_cast<T*>(it.out);
+        DecompPayload<DIM, Tl> P;
+        with_mode(it.mode, [&](auto m) {
+            decompress_load<DIM, decltype(m)::value, Tl>(P, R, pbase);
+            decompress_store<T, DIM, decltype(m)::value, Tl>(P, R, out, g, eb, local);
+        });
+        tile = next;
+        a = an;
+        R = Rn;
+        slot ^= 1;
     }
     finish_cta(hdr, status, total_tiles);
 }

@@ -103,17 +103,21 @@ __device__ __forceinline__ void st_stream(double* p, double v) { __stcs(p, v); }
 
 // ------------------------------------------------------------------ warp bit transpose
 
-// 32x32 bit-matrix transpose across a warp: on entry lane l holds row l (bit b =
-// M[l][b]); on exit lane p holds column p (bit l = M[l][p]).  5 butterfly stages,
-// each one shuffle, one funnel-free shift select and one LOP3.
-__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane)
+// 32x32 bit-matrix transpose across a warp: on entry the lane whose row index is
+// `row` holds row `row` (bit b = M[row][b]); on exit lane p holds column p (bit r =
+// M[r][p]).  5 butterfly stages of one shuffle, one shift select and one LOP3.
+// With row = lane the transpose is the plain one.  With row = lane ^ 7 the element
+// held by lane l lands on bit l ^ 7 of every column word -- the reference's byte
+// layout (8 elements per byte, first element in the most significant bit) -- so a
+// plane word can be stored as it comes out.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int row)
 {
 #pragma unroll
     for (int j = 16; j >= 1; j >>= 1) {
         const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
                          : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
         uint32_t y = __shfl_xor_sync(FULL, x, j);
-        const bool up = lane & j;
+        const bool up = row & j;
         const uint32_t keep = up ? m : ~m;
         const uint32_t sh = up ? (y >> j) : (y << j);
         x = (x & keep) | (sh & ~keep);
@@ -147,10 +151,13 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
 {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p)
+// Status words carry their value (state and prefix in one 64-bit word), so polling
+// needs no acquire ordering; relaxed loads let a lane's polls overlap instead of
+// waiting out one L2 round trip each.
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p)
 {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -161,36 +168,72 @@ __device__ __forceinline__ uint64_t warp_sum64(uint64_t v)
     return v;
 }
 
-// Exclusive prefix of tile `tile` from its predecessors' published words (warp-wide,
-// 32 predecessors per step).  Every wait is bounded: on timeout the error bit is set
-// and the partial sum returned, so no CTA can hang the GPU.
-__device__ __forceinline__ uint64_t lookback(unsigned long long* status, int64_t tile, uint32_t* err, int lane)
+// Exclusive prefix of tile `tile`, looked back by ONE warp over a window of
+// 32 x kLookbackPerLane predecessors per step (poll k reads the 32 consecutive
+// status words hi-32k-31 .. hi-32k, one per lane: coalesced).
+// The newest inclusive prefix in the window ends the walk; every tile newer than it
+// must have posted its aggregate.  A window far wider than a warp matters: a
+// persistent grid keeps hundreds of tiles in flight, and a 32-tile window would need
+// one L2 round trip per 32 of them.  Only warp 0 polls (with exponential back-off);
+// the other warps wait at the caller's barrier and cost no issue slots.
+// Every wait is bounded: on timeout the error bit is set and the partial sum is
+// returned, so no CTA can hang the GPU.
+constexpr int kLookbackPerLane = 8;
+
+struct LookbackShared {
+    unsigned long long excl;
+};
+
+__device__ __forceinline__ uint64_t warp_lookback(unsigned long long* status, int64_t tile, uint32_t* err)
 {
+    const int lane = threadIdx.x & 31;
+    constexpr int K = kLookbackPerLane;
+    constexpr long long NONE = -(1ll << 62);
     uint64_t excl = 0;
-    int64_t base = tile - 1;
-    while (base >= 0) {
-        const int64_t idx = base - lane;
-        unsigned long long w;
+    int64_t hi = tile - 1;
+    while (hi >= 0) {
         int spins = 0;
+        unsigned backoff = 32;
+        unsigned long long w[K];
+        long long jmax;
         while (true) {
-            w = idx >= 0 ? ld_acquire(status + idx) : (unsigned long long)ST_INC;
-            const unsigned pending = __ballot_sync(FULL, (w >> 62) == 0);
-            if (!pending) break;
+            long long j = NONE;
+            bool pend_any = false;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int64_t idx = hi - (int64_t)(k * 32 + lane);
+                w[k] = idx >= 0 ? ld_relaxed(status + idx) : (unsigned long long)ST_INC;   // before tile 0: prefix 0
+            }
+#pragma unroll
+            for (int k = K - 1; k >= 0; k--) {
+                const int64_t idx = hi - (int64_t)(k * 32 + lane);
+                if ((w[k] >> 62) == 2) j = (long long)idx;     // newest inclusive this lane saw
+            }
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) j = max(j, (long long)__shfl_xor_sync(FULL, j, o));
+            jmax = j;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int64_t idx = hi - (int64_t)(k * 32 + lane);
+                pend_any |= (w[k] >> 62) == 0 && (long long)idx > jmax;
+            }
+            if (!__any_sync(FULL, pend_any)) break;
             if (++spins > kSpinLimit) {
                 if (lane == 0) atomicOr(err, ERR_LOOKBACK_TIMEOUT);
                 return excl;
             }
-            __nanosleep(32);
+            __nanosleep(backoff);
+            backoff = backoff < 256 ? 2 * backoff : 256;
         }
-        const unsigned inc = __ballot_sync(FULL, (w >> 62) == 2);
-        uint64_t v = w & ST_VAL;
-        if (inc) {
-            const int k = __ffs(inc) - 1;
-            excl += warp_sum64(lane <= k ? v : 0);
-            return excl;
+        uint64_t v = 0;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int64_t idx = hi - (int64_t)(k * 32 + lane);
+            if (idx >= 0 && (long long)idx >= jmax) v += w[k] & ST_VAL;
         }
         excl += warp_sum64(v);
-        base -= 32;
+        if (jmax != NONE) return excl;
+        hi -= 32 * K;
     }
     return excl;
 }
@@ -217,18 +260,25 @@ __device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* st
     }
 }
 
-// CTA-wide tile prefix: warp totals -> tile aggregate -> publish -> look-back.
-// Returns (through shared memory) the tile's exclusive byte offset and each warp's
-// offset inside the tile; the last tile of an array stores the stream length S in
-// *total_out.  Called by all threads.
+// CTA-wide tile prefix in two halves, so a CTA can issue other work between them:
+//   scan_begin: each warp posts its payload total (then a barrier);
+//   scan_finish: warp 0 scans the totals, publishes the tile aggregate, looks back,
+//                publishes the inclusive prefix (then a barrier).
+// Afterwards s_warp[w] is warp w's offset inside the tile and *s_base the tile's
+// offset inside the payload; the last tile of an array stores S in *total_out.
 template <int WARPS>
-__device__ __forceinline__ void tile_scan(uint32_t warp_total, int64_t tile, uint64_t ntiles,
-                                          unsigned long long* status, uint32_t* err, unsigned long long* total_out,
-                                          uint64_t rate_bytes, uint32_t* s_warp, uint64_t* s_base)
+__device__ __forceinline__ void scan_begin(uint32_t warp_total, uint32_t* s_warp)
+{
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = warp_total;
+    __syncthreads();
+}
+
+template <int WARPS>
+__device__ __forceinline__ void scan_finish(int64_t tile, uint64_t ntiles, unsigned long long* status, uint32_t* err,
+                                            unsigned long long* total_out, uint64_t rate_bytes, uint32_t* s_warp,
+                                            uint64_t* s_base, LookbackShared& lb)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_warp[warp] = warp_total;
-    __syncthreads();
     if (warp == 0) {
         uint32_t v = lane < WARPS ? s_warp[lane] : 0u;
         uint32_t incl = v;
@@ -241,12 +291,9 @@ __device__ __forceinline__ void tile_scan(uint32_t warp_total, int64_t tile, uin
         __syncwarp();
         if (lane < WARPS) s_warp[lane] = incl - v;
         if (lane == 0) st_release(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
-        uint64_t excl = 0;
-        if (tile > 0) {
-            excl = lookback(status, tile, err, lane);
-            if (lane == 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
-        }
+        const uint64_t excl = tile > 0 ? warp_lookback(status, tile, err) : 0;
         if (lane == 0) {
+            if (tile > 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
             *s_base = excl;
             if ((uint64_t)tile == ntiles - 1) *total_out = rate_bytes + excl + agg;
         }

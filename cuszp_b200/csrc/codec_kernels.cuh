@@ -41,13 +41,20 @@ __device__ __forceinline__ void put32(uint8_t* p, uint32_t v)
         *reinterpret_cast<uint32_t*>(p) = v;
     }
 }
+// Outlier-mode payload words sit at any byte offset: read the (at most two) aligned
+// words that hold the four bytes and funnel-shift.  Both aligned words contain bytes
+// of the payload itself, so the reads never leave the pages the stream occupies.
 template <int MODE>
 __device__ __forceinline__ uint32_t get32(const uint8_t* p)
 {
     if constexpr (MODE == MODE_OUTLIER) {
-        return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)3);
+        const uint32_t sh = (uint32_t)(a & 3) * 8;
+        const uint32_t lo = __ldg(w);
+        return sh ? __funnelshift_r(lo, __ldg(w + 1), sh) : lo;
     } else {
-        return *reinterpret_cast<const uint32_t*>(p);
+        return __ldg(reinterpret_cast<const uint32_t*>(p));
     }
 }
 
@@ -67,25 +74,53 @@ __device__ __forceinline__ BlockPos block_pos(uint64_t b, const Geom& g)
     return p;
 }
 
-// Element (half h, lane l) of a 2D/3D block: returns the flat index and validity.
+// Walks a warp's consecutive 2D/3D blocks without per-block divisions: one
+// block_pos() for the first block, then x/y/z carries.  Per-lane element offsets
+// inside a block are fixed for an array.
 template <int DIM>
-__device__ __forceinline__ bool elem_index(const BlockPos& bp, bool block_ok, int h, int lane, const Geom& g,
-                                           uint64_t& idx)
-{
-    uint32_t x, y, z;
-    if constexpr (DIM == 2) {
-        x = bp.x * 8 + (lane & 7);
-        y = bp.y * 8 + (lane >> 3) + 4 * h;
-        z = bp.z;
-    } else {
-        x = bp.x * 4 + (lane & 3);
-        y = bp.y * 4 + ((lane >> 2) & 3);
-        z = bp.z * 4 + (lane >> 4) + 2 * h;
+struct BlockWalk {
+    uint32_t x, y, z;            // block coordinates of the current block
+    uint32_t cx, ry0, ry1, rz0, rz1;
+    uint64_t o0, o1;             // element offsets of this lane's two elements
+
+    __device__ __forceinline__ BlockWalk(uint64_t b0, const Geom& g, int lane)
+    {
+        const BlockPos p = block_pos(b0 < g.nblocks ? b0 : 0, g);
+        x = p.x; y = p.y; z = p.z;
+        if constexpr (DIM == 2) {
+            cx = lane & 7; ry0 = lane >> 3; ry1 = ry0 + 4; rz0 = rz1 = 0;
+            o0 = (uint64_t)ry0 * g.dx + cx;
+            o1 = (uint64_t)ry1 * g.dx + cx;
+        } else {
+            cx = lane & 3; ry0 = ry1 = (lane >> 2) & 3; rz0 = lane >> 4; rz1 = rz0 + 2;
+            o0 = ((uint64_t)rz0 * g.dy + ry0) * g.dx + cx;
+            o1 = ((uint64_t)rz1 * g.dy + ry0) * g.dx + cx;
+        }
     }
-    const bool ok = block_ok && x < g.dx && y < g.dy && z < g.dz;
-    idx = ((uint64_t)z * g.dy + y) * g.dx + x;
-    return ok;
-}
+    // Flat index of this lane's half-0 element and validity of both halves.
+    __device__ __forceinline__ uint64_t elems(const Geom& g, bool bok, bool& ok0, bool& ok1) const
+    {
+        constexpr uint32_t B = DIM == 2 ? 8 : 4;
+        const uint32_t xb = x * B, yb = y * B, zb = DIM == 2 ? z : z * 4;
+        const bool inx = bok && xb + cx < g.dx;
+        if constexpr (DIM == 2) {
+            ok0 = inx && yb + ry0 < g.dy;
+            ok1 = inx && yb + ry1 < g.dy;
+        } else {
+            const bool iny = inx && yb + ry0 < g.dy;
+            ok0 = iny && zb + rz0 < g.dz;
+            ok1 = iny && zb + rz1 < g.dz;
+        }
+        return ((uint64_t)zb * g.dy + yb) * g.dx + xb;
+    }
+    __device__ __forceinline__ void advance(const Geom& g)
+    {
+        if (++x == g.bxn) {
+            x = 0;
+            if (++y == g.byn) { y = 0; ++z; }
+        }
+    }
+};
 
 // Predecessor of each element for the Lorenzo delta (src/cuSZp_kernels_2D_f32.cu:711-760,
 // 3D_f32.cu:697-704): returns q(pred) for half 0 (p0) and half 1 (p1).
@@ -175,386 +210,543 @@ __device__ __forceinline__ void lorenzo_inverse(int32_t& d0, int32_t& d1, int la
     }
 }
 
-// --------------------------------------------------------------- compress
+// --------------------------------------------------------------- compress phases
+//
+// A tile is processed in three phases so that a CTA never idles on its look-back:
+//   load(t+1) is issued right after tile t's aggregate is published, so the DRAM
+//   traffic of the next tile overlaps tile t's look-back and its payload stores.
 
-template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
-__device__ __forceinline__ void compress_tile(const T* __restrict__ in, uint8_t* __restrict__ cmp, const Geom& g,
-                                              T recip, int64_t tile, unsigned long long* __restrict__ status,
-                                              uint32_t* err, unsigned long long* total_out, uint32_t* s_warp,
-                                              uint64_t* s_base)
+template <typename T, int DIM, typename Tl>
+struct CompressIn {
+    T v0[Tl::BPW];
+    T v1[DIM == 1 ? 1 : Tl::BPW];
+    uint32_t ok0, ok1;   // 2D/3D: validity of each block's two elements (bit j)
+};
+
+template <typename T, int DIM, typename Tl>
+struct CompressWork {
+    int32_t c0[Tl::BPW];
+    int32_t c1[DIM == 1 ? 1 : Tl::BPW];
+    uint32_t myrb;    // lane j < BPW: rate byte of the warp's block j
+    uint32_t myoff;   // lane j < BPW: its payload offset inside the warp's range
+    uint32_t wtot;
+};
+
+// Issue the coalesced loads of one tile (one element per lane per block; two in 2D/3D).
+template <typename T, int DIM, typename Tl>
+__device__ __forceinline__ void compress_load(CompressIn<T, DIM, Tl>& L, const T* __restrict__ in, const Geom& g,
+                                              int64_t tile)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * Tl::BPW;
+    if constexpr (DIM == 1) {
+#pragma unroll
+        for (int j = 0; j < Tl::BPW; j++) {
+            const uint64_t i = (b0 + j) * 32 + lane;
+            L.v0[j] = i < g.nbEle ? ld_stream(in + i) : T(0);
+        }
+    } else {
+        BlockWalk<DIM> bw(b0, g, lane);
+        uint32_t m0 = 0, m1 = 0;
+#pragma unroll
+        for (int j = 0; j < Tl::BPW; j++) {
+            bool ok0, ok1;
+            const uint64_t base = bw.elems(g, b0 + j < g.nblocks, ok0, ok1);
+            L.v0[j] = ok0 ? ld_stream(in + base + bw.o0) : T(0);
+            L.v1[j] = ok1 ? ld_stream(in + base + bw.o1) : T(0);
+            m0 |= (uint32_t)ok0 << j;
+            m1 |= (uint32_t)ok1 << j;
+            bw.advance(g);
+        }
+        L.ok0 = m0;
+        L.ok1 = m1;
+    }
+}
+
+// Quantize, predict, reduce block maxima, choose the encoding, write the rate bytes.
+template <typename T, int DIM, int MODE, typename Tl>
+__device__ __forceinline__ void compress_codes(const CompressIn<T, DIM, Tl>& L, CompressWork<T, DIM, Tl>& K, T recip,
+                                               const Geom& g, int64_t tile, uint8_t* __restrict__ cmp)
 {
     constexpr int BPW = Tl::BPW;
     constexpr int W = Tl::W;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    {
-        const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
-
-        // ---- 1. load, quantize, predict
-        int32_t c0[BPW], c1[BPW];
-        if constexpr (DIM == 1) {
-            T v[BPW];
-#pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const uint64_t i = (b0 + j) * 32 + lane;
-                v[j] = i < g.nbEle ? ld_stream(in + i) : T(0);
-            }
-#pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const uint64_t i = (b0 + j) * 32 + lane;
-                const int32_t q = quantize(v[j], recip);
-                int32_t p0 = 0, p1;
-                if constexpr (MODE != MODE_FIXED) predecessors<1>(q, 0, lane, p0, p1);
-                c0[j] = i < g.nbEle ? wsub(q, p0) : 0;
-                c1[j] = 0;
-            }
-        } else {
-            T v0[BPW], v1[BPW];
-            bool ok0[BPW], ok1[BPW];
-#pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const uint64_t b = b0 + j;
-                const bool bok = b < g.nblocks;
-                const BlockPos bp = block_pos(bok ? b : 0, g);
-                uint64_t i0, i1;
-                ok0[j] = elem_index<DIM>(bp, bok, 0, lane, g, i0);
-                ok1[j] = elem_index<DIM>(bp, bok, 1, lane, g, i1);
-                v0[j] = ok0[j] ? ld_stream(in + i0) : T(0);
-                v1[j] = ok1[j] ? ld_stream(in + i1) : T(0);
-            }
-#pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const int32_t q0 = quantize(v0[j], recip), q1 = quantize(v1[j], recip);
-                int32_t p0 = 0, p1 = 0;
-                if constexpr (MODE != MODE_FIXED) predecessors<DIM>(q0, q1, lane, p0, p1);
-                c0[j] = ok0[j] ? wsub(q0, p0) : 0;
-                c1[j] = ok1[j] ? wsub(q1, p1) : 0;
-            }
-        }
-
-        // ---- rate byte per block (block maxima: signed in 1D, unsigned in 2D/3D)
-        uint32_t rb[BPW], off[BPW];
-        uint32_t wtot = 0, myrb = 0;
+    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
+    if constexpr (DIM == 1) {
 #pragma unroll
         for (int j = 0; j < BPW; j++) {
-            const uint32_t a0 = uabs(c0[j]), a1 = uabs(c1[j]);
-            uint32_t m, m2 = 0;
-            if constexpr (DIM == 1) {
-                m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
-                if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
-            } else {
-                m = __reduce_max_sync(FULL, max(a0, a1));
-                if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
-            }
-            const int fr1 = bitlen(m);
-            uint32_t r;
-            if constexpr (MODE == MODE_OUTLIER) {
-                const int fr2 = bitlen(m2);
-                const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
-                const int cost1 = fr1 ? W + fr1 * W : 0;
-                const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
-                r = cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
-            } else {
-                r = (uint32_t)fr1;
-            }
-            rb[j] = r;
-            off[j] = wtot;
-            wtot += payload_size<DIM, MODE>(r);
-            if (lane == j) myrb = r;
+            const uint64_t i = (b0 + j) * 32 + lane;
+            const int32_t q = quantize(L.v0[j], recip);
+            int32_t p0 = 0, p1;
+            if constexpr (MODE != MODE_FIXED) predecessors<1>(q, 0, lane, p0, p1);
+            K.c0[j] = i < g.nbEle ? wsub(q, p0) : 0;
         }
-        if (lane < BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)myrb;
-
-        // ---- 2. tile offset
-        tile_scan<Tl::WARPS>(wtot, tile, g.ntiles, status, err, total_out, g.rate_bytes, s_warp, s_base);
-        uint8_t* const pbase = cmp + g.rate_bytes + *s_base + s_warp[warp];
-
-        // ---- 3. sign maps and bit-planes
+        K.c1[0] = 0;
+    } else {
+#pragma unroll
+        for (int j = 0; j < BPW; j++) {
+            const bool ok0 = (L.ok0 >> j) & 1u, ok1 = (L.ok1 >> j) & 1u;
+            const int32_t q0 = quantize(L.v0[j], recip), q1 = quantize(L.v1[j], recip);
+            int32_t p0 = 0, p1 = 0;
+            if constexpr (MODE != MODE_FIXED) predecessors<DIM>(q0, q1, lane, p0, p1);
+            K.c0[j] = ok0 ? wsub(q0, p0) : 0;
+            K.c1[j] = ok1 ? wsub(q1, p1) : 0;
+        }
+    }
+    // rate byte per block (block maxima: signed in 1D, unsigned in 2D/3D)
+    uint32_t wtot = 0, myrb = 0, myoff = 0;
+#pragma unroll
+    for (int j = 0; j < BPW; j++) {
+        const uint32_t a0 = uabs(K.c0[j]);
+        const uint32_t a1 = DIM == 1 ? 0u : uabs(K.c1[DIM == 1 ? 0 : j]);
+        uint32_t m, m2 = 0;
         if constexpr (DIM == 1) {
-#pragma unroll
-            for (int j = 0; j < BPW; j += 2) {
-                const uint32_t rA = rb[j], rB = rb[j + 1];
-                if ((rA | rB) == 0) continue;
-                uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
-                if constexpr (MODE == MODE_OUTLIER) {
-                    nA = rA & 0x1f; nB = rB & 0x1f;
-                    if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
-                    if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
-                }
-                uint32_t aA = uabs(c0[j]), aB = uabs(c0[j + 1]);
-                uint8_t* pA = pbase + off[j];
-                uint8_t* pB = pbase + off[j + 1];
-                if constexpr (MODE == MODE_OUTLIER) {
-                    if (lane == 0) {
-                        for (uint32_t i = 0; i < obA; i++) pA[i] = (uint8_t)(aA >> (8 * i));
-                        for (uint32_t i = 0; i < obB; i++) pB[i] = (uint8_t)(aB >> (8 * i));
-                        if (obA) aA = 0;
-                        if (obB) aB = 0;
-                    }
-                    pA += obA; pB += obB;
-                }
-                const uint32_t sA = to_stream_word(__ballot_sync(FULL, c0[j] < 0));
-                const uint32_t sB = to_stream_word(__ballot_sync(FULL, c0[j + 1] < 0));
-                const bool hasA = payload_size<DIM, MODE>(rA) != 0, hasB = payload_size<DIM, MODE>(rB) != 0;
-                if (lane == 0 && hasA) put32<MODE>(pA, sA);
-                if (lane == 16 && hasB) put32<MODE>(pB, sB);
-                if (nA <= 16 && nB <= 16) {
-                    const uint32_t y = to_stream_word(warp_transpose32((aA & 0xffffu) | (aB << 16), lane));
-                    const int p = lane & 15;
-                    if (lane < 16) { if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, y); }
-                    else           { if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, y); }
-                } else {
-                    const uint32_t yA = to_stream_word(warp_transpose32(aA, lane));
-                    const uint32_t yB = to_stream_word(warp_transpose32(aB, lane));
-                    if ((uint32_t)lane < nA) put32<MODE>(pA + 4 + 4 * lane, yA);
-                    if ((uint32_t)lane < nB) put32<MODE>(pB + 4 + 4 * lane, yB);
-                }
-            }
+            m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
+            if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
         } else {
+            m = __reduce_max_sync(FULL, max(a0, a1));
+            if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
+        }
+        const int fr1 = bitlen(m);
+        uint32_t r;
+        if constexpr (MODE == MODE_OUTLIER) {
+            const int fr2 = bitlen(m2);
+            const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
+            const int cost1 = fr1 ? W + fr1 * W : 0;
+            const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
+            r = cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
+        } else {
+            r = (uint32_t)fr1;
+        }
+        if (lane == j) { myrb = r; myoff = wtot; }
+        wtot += payload_size<DIM, MODE>(r);
+    }
+    K.wtot = wtot;
+    K.myrb = myrb;
+    K.myoff = myoff;
+    if (lane < BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)myrb;
+}
+
+// Sign maps and bit-planes of the warp's blocks at their final offsets.
+template <typename T, int DIM, int MODE, typename Tl>
+__device__ __forceinline__ void compress_pack(const CompressWork<T, DIM, Tl>& K, uint8_t* __restrict__ pbase)
+{
+    constexpr int BPW = Tl::BPW;
+    const int lane = threadIdx.x & 31;
+    if constexpr (DIM == 1) {
 #pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const uint32_t r = rb[j];
-                if (r == 0) continue;
-                uint32_t n = r, ob = 0;
-                if constexpr (MODE == MODE_OUTLIER) {
-                    n = r & 0x1f;
-                    if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
+        for (int j = 0; j < BPW; j += 2) {
+            const uint32_t rA = __shfl_sync(FULL, K.myrb, j), rB = __shfl_sync(FULL, K.myrb, j + 1);
+            if ((rA | rB) == 0) continue;
+            uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                nA = rA & 0x1f; nB = rB & 0x1f;
+                if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
+                if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
+            }
+            uint32_t aA = uabs(K.c0[j]), aB = uabs(K.c0[j + 1]);
+            uint8_t* pA = pbase + __shfl_sync(FULL, K.myoff, j);
+            uint8_t* pB = pbase + __shfl_sync(FULL, K.myoff, j + 1);
+            if constexpr (MODE == MODE_OUTLIER) {
+                if (lane == 0) {
+                    for (uint32_t i = 0; i < obA; i++) pA[i] = (uint8_t)(aA >> (8 * i));
+                    for (uint32_t i = 0; i < obB; i++) pB[i] = (uint8_t)(aB >> (8 * i));
+                    if (obA) aA = 0;
+                    if (obB) aB = 0;
                 }
-                uint32_t a0 = uabs(c0[j]);
-                const uint32_t a1 = uabs(c1[j]);
-                uint8_t* p = pbase + off[j];
-                if constexpr (MODE == MODE_OUTLIER) {
-                    if (lane == 0) {
-                        for (uint32_t i = 0; i < ob; i++) p[i] = (uint8_t)(a0 >> (8 * i));
-                        if (ob) a0 = 0;
-                    }
-                    p += ob;
+                pA += obA; pB += obB;
+            }
+            const uint32_t sA = to_stream_word(__ballot_sync(FULL, K.c0[j] < 0));
+            const uint32_t sB = to_stream_word(__ballot_sync(FULL, K.c0[j + 1] < 0));
+            const bool hasA = payload_size<DIM, MODE>(rA) != 0, hasB = payload_size<DIM, MODE>(rB) != 0;
+            if (lane == 0 && hasA) put32<MODE>(pA, sA);
+            if (lane == 16 && hasB) put32<MODE>(pB, sB);
+            if (nA <= 16 && nB <= 16) {
+                // lane l holds plane (l ^ 7) & 15 of block A (l < 16) or B (l >= 16)
+                const uint32_t y = warp_transpose32((aA & 0xffffu) | (aB << 16), lane ^ 7);
+                const int p = (lane ^ 7) & 15;
+                if (lane < 16) { if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, y); }
+                else           { if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, y); }
+            } else {
+                const uint32_t yA = warp_transpose32(aA, lane ^ 7);
+                const uint32_t yB = warp_transpose32(aB, lane ^ 7);
+                const int p = lane ^ 7;
+                if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, yA);
+                if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, yB);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < BPW; j++) {
+            const uint32_t r = __shfl_sync(FULL, K.myrb, j);
+            if (r == 0) continue;
+            uint32_t n = r, ob = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                n = r & 0x1f;
+                if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
+            }
+            uint32_t a0 = uabs(K.c0[j]);
+            const uint32_t a1 = uabs(K.c1[DIM == 1 ? 0 : j]);
+            uint8_t* p = pbase + __shfl_sync(FULL, K.myoff, j);
+            if constexpr (MODE == MODE_OUTLIER) {
+                if (lane == 0) {
+                    for (uint32_t i = 0; i < ob; i++) p[i] = (uint8_t)(a0 >> (8 * i));
+                    if (ob) a0 = 0;
                 }
-                const uint32_t s0 = to_stream_word(__ballot_sync(FULL, c0[j] < 0));
-                const uint32_t s1 = to_stream_word(__ballot_sync(FULL, c1[j] < 0));
-                if (lane == 0) put32<MODE>(p, s0);
-                if (lane == 1) put32<MODE>(p + 4, s1);
-                if (n <= 16) {
-                    const uint32_t y = to_stream_word(warp_transpose32((a0 & 0xffffu) | (a1 << 16), lane));
-                    const int pl = lane & 15;
-                    if ((uint32_t)pl < n) put32<MODE>(p + 8 + 8 * pl + (lane >> 4) * 4, y);
-                } else {
-                    const uint32_t ylo = to_stream_word(warp_transpose32(a0, lane));
-                    const uint32_t yhi = to_stream_word(warp_transpose32(a1, lane));
-                    if ((uint32_t)lane < n) {
-                        put32<MODE>(p + 8 + 8 * lane, ylo);
-                        put32<MODE>(p + 12 + 8 * lane, yhi);
-                    }
+                p += ob;
+            }
+            const uint32_t s0 = to_stream_word(__ballot_sync(FULL, K.c0[j] < 0));
+            const uint32_t s1 = to_stream_word(__ballot_sync(FULL, K.c1[DIM == 1 ? 0 : j] < 0));
+            if (lane == 0) put32<MODE>(p, s0);
+            if (lane == 1) put32<MODE>(p + 4, s1);
+            if (n <= 16) {
+                // lane l holds plane (l ^ 7) & 15 of half l >> 4
+                const uint32_t y = warp_transpose32((a0 & 0xffffu) | (a1 << 16), lane ^ 7);
+                const int pl = (lane ^ 7) & 15;
+                if ((uint32_t)pl < n) put32<MODE>(p + 8 + 8 * pl + (lane >> 4) * 4, y);
+            } else {
+                const uint32_t ylo = warp_transpose32(a0, lane ^ 7);
+                const uint32_t yhi = warp_transpose32(a1, lane ^ 7);
+                const int pl = lane ^ 7;
+                if ((uint32_t)pl < n) {
+                    put32<MODE>(p + 8 + 8 * pl, ylo);
+                    put32<MODE>(p + 12 + 8 * pl, yhi);
                 }
             }
         }
     }
 }
 
-template <typename T, int DIM, int MODE>
-__global__ void __launch_bounds__(kThreads)
+// Shared state of one CTA's tile loop.
+template <int WARPS>
+struct TileShared {
+    uint32_t warp[WARPS];
+    uint64_t base;
+    int64_t ticket[2];
+    uint32_t dwarp[2][WARPS];         // decompress: warp offsets of the two tiles in flight
+    unsigned long long dagg[2];       // decompress: their aggregates
+    LookbackShared lb;
+};
+
+// One compress step for tile `tile` (loads already in L): codes -> publish -> issue the
+// loads of tile `next` -> look-back -> pack.  `load_next` issues the next loads.
+template <typename T, int DIM, int MODE, typename Tl, typename LoadNext>
+__device__ __forceinline__ void compress_step(CompressIn<T, DIM, Tl>& L, const Geom& g, T recip, int64_t tile,
+                                              uint8_t* __restrict__ cmp, unsigned long long* __restrict__ status,
+                                              uint32_t* err, unsigned long long* total_out, TileShared<Tl::WARPS>& sh,
+                                              LoadNext&& load_next)
+{
+    CompressWork<T, DIM, Tl> K;
+    compress_codes<T, DIM, MODE, Tl>(L, K, recip, g, tile, cmp);
+    scan_begin<Tl::WARPS>(K.wtot, sh.warp);
+    load_next(L);
+    scan_finish<Tl::WARPS>(tile, g.ntiles, status, err, total_out, g.rate_bytes, sh.warp, &sh.base, sh.lb);
+    compress_pack<T, DIM, MODE, Tl>(K, cmp + g.rate_bytes + sh.base + sh.warp[threadIdx.x >> 5]);
+}
+
+template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
+__global__ void __launch_bounds__(Tl::THREADS, 2)
 compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T recip,
                 WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
 {
-    __shared__ uint32_t s_warp[kWarps];
-    __shared__ uint64_t s_base;
-    __shared__ int64_t s_tile;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
-        __syncthreads();
-        const int64_t tile = s_tile;
-        if ((uint64_t)tile >= g.ntiles) break;
-        compress_tile<T, DIM, MODE>(in, cmp, g, recip, tile, status, &hdr->err, &hdr->total, s_warp, &s_base);
+    __shared__ TileShared<Tl::WARPS> sh;
+    if (threadIdx.x == 0) sh.ticket[0] = (int64_t)atomicAdd(&hdr->ticket, 1u);
+    __syncthreads();
+    int64_t tile = sh.ticket[0];
+    CompressIn<T, DIM, Tl> L;
+    if ((uint64_t)tile < g.ntiles) compress_load<T, DIM, Tl>(L, in, g, tile);
+    for (int it = 1; (uint64_t)tile < g.ntiles; it++) {
+        // the ticket for the next tile is read after the scan's first barrier
+        if (threadIdx.x == 0) sh.ticket[it & 1] = (int64_t)atomicAdd(&hdr->ticket, 1u);
+        int64_t next = 0;
+        compress_step<T, DIM, MODE, Tl>(L, g, recip, tile, cmp, status, &hdr->err, &hdr->total, sh,
+                                        [&](CompressIn<T, DIM, Tl>& Ln) {
+                                            next = sh.ticket[it & 1];
+                                            if ((uint64_t)next < g.ntiles) compress_load<T, DIM, Tl>(Ln, in, g, next);
+                                        });
+        tile = next;
     }
     finish_cta(hdr, status, g.ntiles);
 }
 
-// --------------------------------------------------------------- decompress
+// --------------------------------------------------------------- decompress phases
+//
+// Mirror pipeline: tile t's payload loads are issued, then tile t+1's rate bytes are
+// scanned and looked back (overlapping those loads), then tile t is decoded and stored.
 
-template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
-__device__ __forceinline__ void decompress_tile(T* __restrict__ out, const uint8_t* __restrict__ cmp, const Geom& g,
-                                                T eb, int64_t tile, unsigned long long* __restrict__ status,
-                                                uint32_t* err, unsigned long long* total_out, uint32_t* s_warp,
-                                                uint64_t* s_base)
+template <typename Tl>
+struct DecompRates {
+    uint32_t myrb;    // lane j < BPW: rate byte of block j of this warp
+    uint32_t myoff;   // lane j < BPW: payload offset of block j inside the warp's range
+    uint32_t wtot;
+};
+
+template <int DIM, int MODE, typename Tl>
+__device__ __forceinline__ void decompress_rates(DecompRates<Tl>& R, const uint8_t* __restrict__ cmp, const Geom& g,
+                                                 int64_t tile)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * Tl::BPW;
+    uint32_t myrb = 0;
+    if (lane < Tl::BPW && b0 + lane < g.nblocks) myrb = __ldg(cmp + b0 + lane);
+    const uint32_t sz = lane < Tl::BPW ? payload_size<DIM, MODE>(myrb) : 0u;
+    uint32_t incl = sz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    R.myrb = myrb;
+    R.myoff = incl - sz;
+    R.wtot = __shfl_sync(FULL, incl, 31);
+}
+
+template <int DIM, typename Tl>
+struct DecompPayload {
+    uint32_t w0[Tl::BPW];
+    uint32_t w1[Tl::BPW];
+    uint32_t s0[Tl::BPW];
+    uint32_t s1[DIM == 1 ? 1 : Tl::BPW];
+    uint32_t m0[Tl::BPW];
+};
+
+// Issue the payload loads of the warp's blocks (plane words, sign words, outlier bytes).
+template <int DIM, int MODE, typename Tl>
+__device__ __forceinline__ void decompress_load(DecompPayload<DIM, Tl>& P, const DecompRates<Tl>& R,
+                                                const uint8_t* __restrict__ pbase)
 {
     constexpr int BPW = Tl::BPW;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    {
-        const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
-
-        // ---- rate bytes -> payload sizes -> warp-local offsets
-        uint32_t myrb = 0;
-        if (lane < BPW && b0 + lane < g.nblocks) myrb = cmp[b0 + lane];
-        const uint32_t sz = lane < BPW ? payload_size<DIM, MODE>(myrb) : 0u;
-        uint32_t incl = sz;
+    const int lane = threadIdx.x & 31;
+    if constexpr (DIM == 1) {
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += t;
+        for (int k = 0; k < BPW / 2; k++) {
+            const int j = 2 * k;
+            const uint32_t rA = __shfl_sync(FULL, R.myrb, j), rB = __shfl_sync(FULL, R.myrb, j + 1);
+            const uint32_t oA = __shfl_sync(FULL, R.myoff, j), oB = __shfl_sync(FULL, R.myoff, j + 1);
+            uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                nA = rA & 0x1f; nB = rB & 0x1f;
+                if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
+                if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
+            }
+            const uint8_t* pA = pbase + oA;
+            const uint8_t* pB = pbase + oB;
+            P.m0[j] = 0; P.m0[j + 1] = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                for (uint32_t i = 0; i < obA; i++) P.m0[j] |= (uint32_t)pA[i] << (8 * i);
+                for (uint32_t i = 0; i < obB; i++) P.m0[j + 1] |= (uint32_t)pB[i] << (8 * i);
+                pA += obA; pB += obB;
+            }
+            const bool hasA = payload_size<DIM, MODE>(rA) != 0, hasB = payload_size<DIM, MODE>(rB) != 0;
+            P.s0[j] = hasA ? get32<MODE>(pA) : 0u;
+            P.s0[j + 1] = hasB ? get32<MODE>(pB) : 0u;
+            P.w0[k] = 0; P.w1[k] = 0;
+            if (nA <= 16 && nB <= 16) {
+                const int p = lane & 15;
+                if (lane < 16) { if ((uint32_t)p < nA) P.w0[k] = get32<MODE>(pA + 4 + 4 * p); }
+                else           { if ((uint32_t)p < nB) P.w0[k] = get32<MODE>(pB + 4 + 4 * p); }
+            } else {
+                if ((uint32_t)lane < nA) P.w0[k] = get32<MODE>(pA + 4 + 4 * lane);
+                if ((uint32_t)lane < nB) P.w1[k] = get32<MODE>(pB + 4 + 4 * lane);
+            }
         }
-        const uint32_t myoff = incl - sz;
-        const uint32_t wtot = __shfl_sync(FULL, incl, 31);
-
-        tile_scan<Tl::WARPS>(wtot, tile, g.ntiles, status, err, total_out, g.rate_bytes, s_warp, s_base);
-        const uint8_t* const pbase = cmp + g.rate_bytes + *s_base + s_warp[warp];
-
-        if constexpr (DIM == 1) {
-            // ---- load phase: plane words and sign words of all blocks
-            constexpr int NP = BPW / 2;
-            uint32_t wA[NP], wB[NP], sgA[NP], sgB[NP], m0A[NP], m0B[NP];
+    } else {
 #pragma unroll
-            for (int k = 0; k < NP; k++) {
-                const int j = 2 * k;
-                const uint32_t rA = __shfl_sync(FULL, myrb, j), rB = __shfl_sync(FULL, myrb, j + 1);
-                const uint32_t oA = __shfl_sync(FULL, myoff, j), oB = __shfl_sync(FULL, myoff, j + 1);
-                uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
-                if constexpr (MODE == MODE_OUTLIER) {
-                    nA = rA & 0x1f; nB = rB & 0x1f;
-                    if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
-                    if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
-                }
-                const uint8_t* pA = pbase + oA;
-                const uint8_t* pB = pbase + oB;
-                m0A[k] = 0; m0B[k] = 0;
-                if constexpr (MODE == MODE_OUTLIER) {
-                    for (uint32_t i = 0; i < obA; i++) m0A[k] |= (uint32_t)pA[i] << (8 * i);
-                    for (uint32_t i = 0; i < obB; i++) m0B[k] |= (uint32_t)pB[i] << (8 * i);
-                    pA += obA; pB += obB;
-                }
-                const bool hasA = payload_size<DIM, MODE>(rA) != 0, hasB = payload_size<DIM, MODE>(rB) != 0;
-                sgA[k] = hasA ? get32<MODE>(pA) : 0u;
-                sgB[k] = hasB ? get32<MODE>(pB) : 0u;
-                wA[k] = 0; wB[k] = 0;
-                if (nA <= 16 && nB <= 16) {
-                    const int p = lane & 15;
-                    if (lane < 16) { if ((uint32_t)p < nA) wA[k] = get32<MODE>(pA + 4 + 4 * p); }
-                    else           { if ((uint32_t)p < nB) wA[k] = get32<MODE>(pB + 4 + 4 * p); }
-                } else {
-                    if ((uint32_t)lane < nA) wA[k] = get32<MODE>(pA + 4 + 4 * lane);
-                    if ((uint32_t)lane < nB) wB[k] = get32<MODE>(pB + 4 + 4 * lane);
-                }
+        for (int j = 0; j < BPW; j++) {
+            const uint32_t r = __shfl_sync(FULL, R.myrb, j);
+            const uint32_t o = __shfl_sync(FULL, R.myoff, j);
+            uint32_t n = r, ob = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                n = r & 0x1f;
+                if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
             }
-            // ---- decode phase: one warp transpose per pair (two if a rate exceeds 16)
-#pragma unroll
-            for (int k = 0; k < NP; k++) {
-                const uint32_t rA = __shfl_sync(FULL, myrb, 2 * k), rB = __shfl_sync(FULL, myrb, 2 * k + 1);
-                uint32_t nA = rA, nB = rB;
-                if constexpr (MODE == MODE_OUTLIER) { nA = rA & 0x1f; nB = rB & 0x1f; }
-                uint32_t magA = 0, magB = 0;
-                if (nA <= 16 && nB <= 16) {
-                    if ((nA | nB) != 0) {
-                        const uint32_t x = warp_transpose32(from_stream_word(wA[k]), lane);
-                        magA = x & 0xffffu;
-                        magB = x >> 16;
-                    }
-                } else {
-                    magA = warp_transpose32(from_stream_word(wA[k]), lane);
-                    magB = warp_transpose32(from_stream_word(wB[k]), lane);
-                }
-                if constexpr (MODE == MODE_OUTLIER) {
-                    if (lane == 0) {
-                        if (rA & 0x80) magA = m0A[k];
-                        if (rB & 0x80) magB = m0B[k];
-                    }
-                }
-#pragma unroll
-                for (int s = 0; s < 2; s++) {
-                    const uint32_t r = s ? rB : rA;
-                    const uint64_t i = (b0 + 2 * k + s) * 32 + lane;
-                    if (payload_size<DIM, MODE>(r) == 0) {
-                        if (i < g.nbEle) st_stream(out + i, T(0));
-                        continue;
-                    }
-                    const uint32_t mag = s ? magB : magA;
-                    const uint32_t sg = from_stream_word(s ? sgB[k] : sgA[k]);
-                    int32_t d = ((sg >> lane) & 1u) ? (int32_t)(0u - mag) : (int32_t)mag;
-                    int32_t dummy = 0;
-                    if constexpr (MODE != MODE_FIXED) lorenzo_inverse<1>(d, dummy, lane);
-                    if (i < g.nbEle) st_stream(out + i, dequant(d, eb));
-                }
+            const uint8_t* p = pbase + o;
+            P.m0[j] = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                for (uint32_t i = 0; i < ob; i++) P.m0[j] |= (uint32_t)p[i] << (8 * i);
+                p += ob;
             }
-        } else {
-            // ---- load phase
-            uint32_t w0[BPW], w1[BPW], sg0[BPW], sg1[BPW], m0[BPW];
-#pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const uint32_t r = __shfl_sync(FULL, myrb, j);
-                const uint32_t o = __shfl_sync(FULL, myoff, j);
-                uint32_t n = r, ob = 0;
-                if constexpr (MODE == MODE_OUTLIER) {
-                    n = r & 0x1f;
-                    if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
-                }
-                const uint8_t* p = pbase + o;
-                m0[j] = 0;
-                if constexpr (MODE == MODE_OUTLIER) {
-                    for (uint32_t i = 0; i < ob; i++) m0[j] |= (uint32_t)p[i] << (8 * i);
-                    p += ob;
-                }
-                const bool has = payload_size<DIM, MODE>(r) != 0;
-                sg0[j] = has ? get32<MODE>(p) : 0u;
-                sg1[j] = has ? get32<MODE>(p + 4) : 0u;
-                w0[j] = 0; w1[j] = 0;
-                if (n <= 16) {
-                    const int pl = lane & 15;
-                    if ((uint32_t)pl < n) w0[j] = get32<MODE>(p + 8 + 8 * pl + (lane >> 4) * 4);
-                } else if ((uint32_t)lane < n) {
-                    w0[j] = get32<MODE>(p + 8 + 8 * lane);
-                    w1[j] = get32<MODE>(p + 12 + 8 * lane);
-                }
-            }
-            // ---- decode phase
-#pragma unroll
-            for (int j = 0; j < BPW; j++) {
-                const uint64_t b = b0 + j;
-                const bool bok = b < g.nblocks;
-                const BlockPos bp = block_pos(bok ? b : 0, g);
-                uint64_t i0, i1;
-                const bool ok0 = elem_index<DIM>(bp, bok, 0, lane, g, i0);
-                const bool ok1 = elem_index<DIM>(bp, bok, 1, lane, g, i1);
-                const uint32_t r = __shfl_sync(FULL, myrb, j);
-                if (payload_size<DIM, MODE>(r) == 0) {
-                    if (ok0) st_stream(out + i0, T(0));
-                    if (ok1) st_stream(out + i1, T(0));
-                    continue;
-                }
-                uint32_t n = r;
-                if constexpr (MODE == MODE_OUTLIER) n = r & 0x1f;
-                uint32_t mag0, mag1;
-                if (n <= 16) {
-                    const uint32_t x = warp_transpose32(from_stream_word(w0[j]), lane);
-                    mag0 = x & 0xffffu;
-                    mag1 = x >> 16;
-                } else {
-                    mag0 = warp_transpose32(from_stream_word(w0[j]), lane);
-                    mag1 = warp_transpose32(from_stream_word(w1[j]), lane);
-                }
-                if constexpr (MODE == MODE_OUTLIER) {
-                    if ((r & 0x80) && lane == 0) mag0 = m0[j];
-                }
-                const uint32_t s0 = from_stream_word(sg0[j]), s1 = from_stream_word(sg1[j]);
-                int32_t d0 = ((s0 >> lane) & 1u) ? (int32_t)(0u - mag0) : (int32_t)mag0;
-                int32_t d1 = ((s1 >> lane) & 1u) ? (int32_t)(0u - mag1) : (int32_t)mag1;
-                if constexpr (MODE != MODE_FIXED) lorenzo_inverse<DIM>(d0, d1, lane);
-                if (ok0) st_stream(out + i0, dequant(d0, eb));
-                if (ok1) st_stream(out + i1, dequant(d1, eb));
+            const bool has = payload_size<DIM, MODE>(r) != 0;
+            P.s0[j] = has ? get32<MODE>(p) : 0u;
+            P.s1[j] = has ? get32<MODE>(p + 4) : 0u;
+            P.w0[j] = 0; P.w1[j] = 0;
+            if (n <= 16) {
+                const int pl = lane & 15;
+                if ((uint32_t)pl < n) P.w0[j] = get32<MODE>(p + 8 + 8 * pl + (lane >> 4) * 4);
+            } else if ((uint32_t)lane < n) {
+                P.w0[j] = get32<MODE>(p + 8 + 8 * lane);
+                P.w1[j] = get32<MODE>(p + 12 + 8 * lane);
             }
         }
     }
 }
 
-template <typename T, int DIM, int MODE>
-__global__ void __launch_bounds__(kThreads)
+// Inverse transpose, signs, inverse Lorenzo, dequantize, store.
+template <typename T, int DIM, int MODE, typename Tl>
+__device__ __forceinline__ void decompress_store(const DecompPayload<DIM, Tl>& P, const DecompRates<Tl>& R,
+                                                 T* __restrict__ out, const Geom& g, T eb, int64_t tile)
+{
+    constexpr int BPW = Tl::BPW;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
+    if constexpr (DIM == 1) {
+#pragma unroll
+        for (int k = 0; k < BPW / 2; k++) {
+            const uint32_t rA = __shfl_sync(FULL, R.myrb, 2 * k), rB = __shfl_sync(FULL, R.myrb, 2 * k + 1);
+            uint32_t nA = rA, nB = rB;
+            if constexpr (MODE == MODE_OUTLIER) { nA = rA & 0x1f; nB = rB & 0x1f; }
+            uint32_t magA = 0, magB = 0;
+            if (nA <= 16 && nB <= 16) {
+                if ((nA | nB) != 0) {
+                    const uint32_t x = warp_transpose32(from_stream_word(P.w0[k]), lane);
+                    magA = x & 0xffffu;
+                    magB = x >> 16;
+                }
+            } else {
+                magA = warp_transpose32(from_stream_word(P.w0[k]), lane);
+                magB = warp_transpose32(from_stream_word(P.w1[k]), lane);
+            }
+            if constexpr (MODE == MODE_OUTLIER) {
+                if (lane == 0) {
+                    if (rA & 0x80) magA = P.m0[2 * k];
+                    if (rB & 0x80) magB = P.m0[2 * k + 1];
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const uint32_t r = s ? rB : rA;
+                const uint64_t i = (b0 + 2 * k + s) * 32 + lane;
+                if (payload_size<DIM, MODE>(r) == 0) {
+                    if (i < g.nbEle) st_stream(out + i, T(0));
+                    continue;
+                }
+                const uint32_t mag = s ? magB : magA;
+                const uint32_t sg = from_stream_word(P.s0[2 * k + s]);
+                int32_t d = ((sg >> lane) & 1u) ? (int32_t)(0u - mag) : (int32_t)mag;
+                int32_t dummy = 0;
+                if constexpr (MODE != MODE_FIXED) lorenzo_inverse<1>(d, dummy, lane);
+                if (i < g.nbEle) st_stream(out + i, dequant(d, eb));
+            }
+        }
+    } else {
+        BlockWalk<DIM> bw(b0, g, lane);
+#pragma unroll
+        for (int j = 0; j < BPW; j++) {
+            bool ok0, ok1;
+            const uint64_t base = bw.elems(g, b0 + j < g.nblocks, ok0, ok1);
+            bw.advance(g);
+            const uint64_t i0 = base + bw.o0, i1 = base + bw.o1;
+            const uint32_t r = __shfl_sync(FULL, R.myrb, j);
+            if (payload_size<DIM, MODE>(r) == 0) {
+                if (ok0) st_stream(out + i0, T(0));
+                if (ok1) st_stream(out + i1, T(0));
+                continue;
+            }
+            uint32_t n = r;
+            if constexpr (MODE == MODE_OUTLIER) n = r & 0x1f;
+            uint32_t mag0, mag1;
+            if (n <= 16) {
+                const uint32_t x = warp_transpose32(from_stream_word(P.w0[j]), lane);
+                mag0 = x & 0xffffu;
+                mag1 = x >> 16;
+            } else {
+                mag0 = warp_transpose32(from_stream_word(P.w0[j]), lane);
+                mag1 = warp_transpose32(from_stream_word(P.w1[j]), lane);
+            }
+            if constexpr (MODE == MODE_OUTLIER) {
+                if ((r & 0x80) && lane == 0) mag0 = P.m0[j];
+            }
+            const uint32_t s0 = from_stream_word(P.s0[j]), s1 = from_stream_word(P.s1[DIM == 1 ? 0 : j]);
+            int32_t d0 = ((s0 >> lane) & 1u) ? (int32_t)(0u - mag0) : (int32_t)mag0;
+            int32_t d1 = ((s1 >> lane) & 1u) ? (int32_t)(0u - mag1) : (int32_t)mag1;
+            if constexpr (MODE != MODE_FIXED) lorenzo_inverse<DIM>(d0, d1, lane);
+            if (ok0) st_stream(out + i0, dequant(d0, eb));
+            if (ok1) st_stream(out + i1, dequant(d1, eb));
+        }
+    }
+}
+
+// Posts a tile's aggregate as soon as its rate bytes are scanned -- before any
+// waiting -- so that no tile ever waits on a predecessor that is itself waiting.
+template <int WARPS>
+__device__ __forceinline__ void post_aggregate(uint32_t warp_total, int64_t tile, unsigned long long* status,
+                                               uint32_t* s_w, unsigned long long* s_agg)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_w[warp] = warp_total;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = lane < WARPS ? s_w[lane] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < WARPS; o <<= 1) {
+            uint32_t t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const uint64_t agg = __shfl_sync(FULL, incl, WARPS - 1);
+        __syncwarp();
+        if (lane < WARPS) s_w[lane] = incl - v;
+        if (lane == 0) {
+            st_release(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
+            *s_agg = agg;
+        }
+    }
+    __syncthreads();
+}
+
+// Look-back for a tile whose aggregate was posted earlier (warp 0 polls, the CTA
+// waits at one barrier); returns its exclusive payload offset in every thread and
+// publishes its inclusive prefix.
+template <int WARPS>
+__device__ __forceinline__ uint64_t resolve_tile(int64_t tile, uint64_t ntiles, unsigned long long* status,
+                                                 uint32_t* err, unsigned long long* total_out, uint64_t rate_bytes,
+                                                 unsigned long long agg, LookbackShared& lb)
+{
+    if ((threadIdx.x >> 5) == 0) {
+        const uint64_t excl = tile > 0 ? warp_lookback(status, tile, err) : 0;
+        if (threadIdx.x == 0) {
+            if (tile > 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
+            if ((uint64_t)tile == ntiles - 1) *total_out = rate_bytes + excl + agg;
+            lb.excl = excl;
+        }
+    }
+    __syncthreads();
+    return lb.excl;
+}
+
+template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
+__global__ void __launch_bounds__(Tl::THREADS, 2)
 decompress_kernel(T* __restrict__ out, const uint8_t* __restrict__ cmp, Geom g, T eb,
                   WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
 {
-    __shared__ uint32_t s_warp[kWarps];
-    __shared__ uint64_t s_base;
-    __shared__ int64_t s_tile;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&hdr->ticket, 1u);
+    __shared__ TileShared<Tl::WARPS> sh;
+    if (threadIdx.x == 0) sh.ticket[0] = (int64_t)atomicAdd(&hdr->ticket, 1u);
+    __syncthreads();
+    int64_t tile = sh.ticket[0];
+    int slot = 0;
+    DecompRates<Tl> R;
+    if ((uint64_t)tile < g.ntiles) {
+        decompress_rates<DIM, MODE, Tl>(R, cmp, g, tile);
+        post_aggregate<Tl::WARPS>(R.wtot, tile, status, sh.dwarp[0], &sh.dagg[0]);
+    }
+    for (int it = 1; (uint64_t)tile < g.ntiles; it++) {
+        if (threadIdx.x == 0) sh.ticket[it & 1] = (int64_t)atomicAdd(&hdr->ticket, 1u);
         __syncthreads();
-        const int64_t tile = s_tile;
-        if ((uint64_t)tile >= g.ntiles) break;
-        decompress_tile<T, DIM, MODE>(out, cmp, g, eb, tile, status, &hdr->err, &hdr->total, s_warp, &s_base);
+        const int64_t next = sh.ticket[it & 1];
+        DecompRates<Tl> Rn = R;
+        if ((uint64_t)next < g.ntiles) {
+            decompress_rates<DIM, MODE, Tl>(Rn, cmp, g, next);
+            post_aggregate<Tl::WARPS>(Rn.wtot, next, status, sh.dwarp[slot ^ 1], &sh.dagg[slot ^ 1]);
+        }
+        const uint64_t excl = resolve_tile<Tl::WARPS>(tile, g.ntiles, status, &hdr->err, &hdr->total, g.rate_bytes,
+                                                      sh.dagg[slot], sh.lb);
+        const uint8_t* pbase = cmp + g.rate_bytes + excl + sh.dwarp[slot][threadIdx.x >> 5];
+        DecompPayload<DIM, Tl> P;
+        decompress_load<DIM, MODE, Tl>(P, R, pbase);
+        decompress_store<T, DIM, MODE, Tl>(P, R, out, g, eb, tile);
+        tile = next;
+        R = Rn;
+        slot ^= 1;
     }
     finish_cta(hdr, status, g.ntiles);
 }
