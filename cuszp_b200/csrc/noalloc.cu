@@ -1,0 +1,171 @@
+// noalloc.cu -- a compression entry point that allocates nothing.
+//
+// Every other entry point needs device scratch for the look-back (a small header and
+// one status word per tile), either from the caller (cuSZp_*_async) or from the
+// stream-ordered pool (cuSZp_compress / _ex).  Some callers cannot provide either:
+// code running where allocation is forbidden or would stall -- inside a region whose
+// owner reserved all device memory up front, a real-time loop that must never hit an
+// allocator, a plugin hosted by a framework that owns the device heap.  For them,
+// cuSZp_compress_noalloc takes its scratch from one fixed array compiled into this
+// library (kNoAllocScratchBytes per device; every GPU that loads the library holds it
+// until the process exits).  The caller still passes the input, the output buffer and
+// a device word for the stream length.
+//
+// The array is shared by every call on a device: calls whose kernels overlap on the
+// GPU (different streams, no ordering) race on it and must not be issued.  It keeps
+// the last call's contents, so each call clears the part it uses before launching.
+#include "../../include/cuSZp.h"
+#include "codec_kernels.cuh"
+#include "codec_launch.cuh"
+
+#include <cstdio>
+#include <mutex>
+
+namespace cuszp {
+
+// 1 MiB: a 48-byte header plus 131,066 tile-status words, i.e. arrays of up to
+// 536,805,376 elements in 1D (4,096 elements per tile) and the same number of
+// elements in 2D/3D (64 blocks of 64 elements per tile).
+constexpr size_t kNoAllocScratchBytes = 1u << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Same tile loop as compress_kernel, on scratch at `ws`; the stream length goes to
+// *size_out, or ~0 when a bounded look-back wait gave up.
+template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
+__global__ void __launch_bounds__(Tl::THREADS, 2)
+compress_noalloc_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T recip, unsigned char* ws,
+                        unsigned long long* __restrict__ size_out)
+{
+    WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(ws + sizeof(WsHeader));
+    __shared__ TileShared<Tl::WARPS> sh;
+    if (threadIdx.x == 0) sh.ticket[0] = (int64_t)atomicAdd(&hdr->ticket, 1u);
+    __syncthreads();
+    int64_t tile = sh.ticket[0];
+    CompressIn<T, DIM, Tl> L;
+    if ((uint64_t)tile < g.ntiles) compress_load<T, DIM, Tl>(L, in, g, tile);
+    for (int it = 1; (uint64_t)tile < g.ntiles; it++) {
+        if (threadIdx.x == 0) sh.ticket[it & 1] = (int64_t)atomicAdd(&hdr->ticket, 1u);
+        int64_t next = 0;
+        compress_step<T, DIM, MODE, Tl>(L, g, recip, tile, cmp, status, &hdr->err, size_out, sh,
+                                        [&](CompressIn<T, DIM, Tl>& Ln) {
+                                            next = sh.ticket[it & 1];
+                                            if ((uint64_t)next < g.ntiles) compress_load<T, DIM, Tl>(Ln, in, g, next);
+                                        });
+        tile = next;
+    }
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&hdr->done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        if (hdr->err) *size_out = ~0ull;
+    }
+}
+
+namespace {
+
+template <typename T, int DIM>
+const void* pick_noalloc(int mode)
+{
+    if (mode == 0) return (const void*)compress_noalloc_kernel<T, DIM, 0>;
+    if (mode == 1) return (const void*)compress_noalloc_kernel<T, DIM, 1>;
+    return (const void*)compress_noalloc_kernel<T, DIM, 2>;
+}
+
+const void* noalloc_kernel(const Problem& p)
+{
+    if (p.type == 0) {
+        if (p.dim == 1) return pick_noalloc<float, 1>(p.mode);
+        if (p.dim == 2) return pick_noalloc<float, 2>(p.mode);
+        return pick_noalloc<float, 3>(p.mode);
+    }
+    if (p.dim == 1) return pick_noalloc<double, 1>(p.mode);
+    if (p.dim == 2) return pick_noalloc<double, 2>(p.mode);
+    return pick_noalloc<double, 3>(p.mode);
+}
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned char* g_scratch_addr[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};
+
+// Once per device, with that device current: the array's device address (in host
+// code the symbol itself is only a host-side stand-in) and the SM count.
+int device_setup(int dev, unsigned char** addr, int* sms)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            std::fprintf(stderr, "cuSZp_compress_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+                         cudaGetErrorString(e));
+            return E_CUDA;
+        }
+        if (cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return E_CUDA;
+        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *addr = g_scratch_addr[dev];
+    *sms = g_sms[dev];
+    return OK;
+}
+
+}  // namespace
+}  // namespace cuszp
+
+using namespace cuszp;
+
+extern "C" int cuSZp_compress_noalloc(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
+                                      float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
+                                      cuszp_mode_t mode, unsigned long long* d_cmpSize, cudaStream_t stream)
+{
+    if (!d_cmpSize) return E_ARG;
+    Problem p;
+    int st = make_problem(p, type, mode, dim, nbEle, dims.x, dims.y, dims.z);
+    if (st) return st;
+    if (p.g.ntiles == 0) {   // empty stream: length 0, nothing to launch
+        return cudaMemsetAsync(d_cmpSize, 0, sizeof(unsigned long long), stream) == cudaSuccess ? OK : E_CUDA;
+    }
+    if (!d_oriData || !d_cmpBytes) return E_ARG;
+    if ((uintptr_t)d_oriData % (type == CUSZP_TYPE_FLOAT ? 4 : 8)) return E_ARG;
+    if (mode != CUSZP_MODE_OUTLIER && (uintptr_t)d_cmpBytes % 4) return E_ARG;
+    const size_t need = workspace_bytes(p);
+    if (need > kNoAllocScratchBytes) {
+        std::fprintf(stderr,
+                     "cuSZp_compress_noalloc: this array needs %llu tiles of look-back state (%zu bytes); the "
+                     "built-in scratch holds %llu tiles (%zu bytes). Use cuSZp_compress_async with a workspace.\n",
+                     (unsigned long long)p.g.ntiles, need,
+                     (unsigned long long)((kNoAllocScratchBytes - sizeof(WsHeader)) / 8), kNoAllocScratchBytes);
+        return E_WORKSPACE;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return E_CUDA;
+    unsigned char* ws = nullptr;
+    int sms = 0;
+    if ((st = device_setup(dev, &ws, &sms))) return st;
+    // a previous call may have been aborted mid-way: start from zero
+    if (cudaMemsetAsync(ws, 0, need, stream) != cudaSuccess) return E_CUDA;
+    const void* fn = noalloc_kernel(p);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, 0);
+    if (occ < 1) occ = 1;
+    const uint64_t want = (uint64_t)sms * occ;
+    const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
+    Geom g = p.g;
+    float rf = 0.5f / errorBound;
+    double rd = 0.5 / (double)errorBound;
+    void* args[6];
+    args[0] = (void*)&d_oriData;
+    args[1] = (void*)&d_cmpBytes;
+    args[2] = (void*)&g;
+    args[3] = type == CUSZP_TYPE_FLOAT ? (void*)&rf : (void*)&rd;
+    args[4] = (void*)&ws;
+    args[5] = (void*)&d_cmpSize;
+    return cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, 0, stream) == cudaSuccess ? OK : E_CUDA;
+}

@@ -190,6 +190,22 @@ void cuSZp_batch_plan_destroy(cuszp_batch_plan_t plan);
 /* Release a plan once the work already enqueued on `stream` is done (stream-ordered free). */
 void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t plan, cudaStream_t stream);
 
+/* Compression without any allocation -- no counterpart in the reference.  For callers
+ * that cannot allocate device memory when they compress (allocation forbidden or too
+ * slow where they run, or all memory owned by a host framework): the look-back scratch
+ * is a fixed 1 MiB array inside this library on each device, so the call allocates
+ * nothing and needs no workspace.  Limit: arrays of at most 131,066 tiles (536,805,376
+ * elements; 4,096 elements per tile); larger arrays are rejected with
+ * CUSZP_ERROR_WORKSPACE and a message on stderr.  Asynchronous on `stream`; the stream
+ * length goes to *d_cmpSize (device uint64, required), or ~0 if a bounded device-side
+ * wait gave up.  The first call on a device looks up the array's device address; make
+ * that first call before any stream capture.  All calls on a device share the array:
+ * calls that can overlap on the GPU race and must be ordered (same stream or explicit
+ * dependencies).  Output bytes are identical to cuSZp_compress_async's. */
+int cuSZp_compress_noalloc(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
+                           float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
+                           cuszp_mode_t mode, unsigned long long* d_cmpSize, cudaStream_t stream);
+
 /* Version string of this build. */
 const char* cuSZp_version(void);
 
