@@ -115,48 +115,57 @@ __device__ __forceinline__ void take_ticket(TileShared<WARPS>& sh, uint32_t* s_i
     s_item[k] = (uint64_t)t < total_tiles ? tile_map[t] : 0u;
 }
 
+// Tile source over the arrays of a batch: tickets index the global tile sequence,
+// the tile map names the array, each array has its own status words and bound.
+template <typename T, int DIM, typename Tl>
+struct BatchSource {
+    const BatchItem* items;
+    const uint32_t* tile_map;
+    uint64_t total_tiles;
+    WsHeader* hdr;
+    unsigned long long* status;
+    unsigned long long* sizes;
+    __device__ __forceinline__ void take(PipeShared<Tl::WARPS>& sp, int k)
+    {
+        const int64_t t = (int64_t)atomicAdd(&hdr->ticket, 1u);
+        sp.ticket[k] = t;
+        sp.item[k] = (uint64_t)t < total_tiles ? tile_map[t] : 0u;
+    }
+    __device__ __forceinline__ bool ctx(const PipeShared<Tl::WARPS>& sp, int k, TileCtx& c) const
+    {
+        const int64_t t = sp.ticket[k];
+        if ((uint64_t)t >= total_tiles) return false;
+        const uint32_t a = sp.item[k];
+        const BatchItem& it = items[a];
+        c.in = it.in;
+        c.cmp = static_cast<uint8_t*>(it.out);
+        c.g = it.g;
+        c.status = status + it.tile_start;
+        c.total_out = sizes + a;
+        c.local = t - (int64_t)it.tile_start;
+        c.mode = it.mode;
+        c.eb = it.eb;
+        return true;
+    }
+    __device__ __forceinline__ unsigned long long encode(const T* buf, uint32_t ok0, uint32_t ok1, const TileCtx& c,
+                                                         uint8_t* sb, PipeShared<Tl::WARPS>& sp) const
+    {
+        const T recip = recip_of<T>(c.eb);
+        unsigned long long agg = 0;
+        with_mode(c.mode, [&](auto m) { agg = encode_tile<T, DIM, decltype(m)::value, Tl>(buf, ok0, ok1, c, recip, sb, sp); });
+        return agg;
+    }
+};
+
 template <typename T, int DIM, typename Tl>
 __global__ void __launch_bounds__(Tl::THREADS, 512 / Tl::THREADS > 0 ? 512 / Tl::THREADS : 1)
 compress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
                       uint64_t total_tiles, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status,
                       unsigned long long* __restrict__ sizes)
 {
-    __shared__ TileShared<Tl::WARPS> sh;
-    __shared__ uint32_t s_item[2];
-    if (threadIdx.x == 0) take_ticket<Tl::WARPS>(sh, s_item, 0, hdr, tile_map, total_tiles);
-    __syncthreads();
-    int64_t tile = sh.ticket[0];
-    uint32_t a = s_item[0];
-    CompressIn<T, DIM, Tl> L;
-    if ((uint64_t)tile < total_tiles) {
-        const BatchItem& it = items[a];
-        compress_load<T, DIM, Tl>(L, static_cast<const T*>(it.in), it.g, tile - (int64_t)it.tile_start);
-    }
-    for (int k = 1; (uint64_t)tile < total_tiles; k++) {
-        if (threadIdx.x == 0) take_ticket<Tl::WARPS>(sh, s_item, k & 1, hdr, tile_map, total_tiles);
-        const BatchItem& it = items[a];
-        const Geom g = it.g;
-        const int64_t local = tile - (int64_t)it.tile_start;
-        const T recip = recip_of<T>(it.eb);
-        uint8_t* out = static_cast<uint8_t*>(it.out);
-        unsigned long long* st = status + it.tile_start;
-        int64_t next = 0;
-        uint32_t an = 0;
-        auto load_next = [&](CompressIn<T, DIM, Tl>& Ln) {
-            next = sh.ticket[k & 1];
-            an = s_item[k & 1];
-            if ((uint64_t)next < total_tiles) {
-                const BatchItem& itn = items[an];
-                compress_load<T, DIM, Tl>(Ln, static_cast<const T*>(itn.in), itn.g, next - (int64_t)itn.tile_start);
-            }
-        };
-        with_mode(it.mode, [&](auto m) {
-            compress_step<T, DIM, decltype(m)::value, Tl>(L, g, recip, local, out, st, &hdr->err, sizes + a, sh,
-                                                          load_next);
-        });
-        tile = next;
-        a = an;
-    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSource<T, DIM, Tl> src{items, tile_map, total_tiles, hdr, status, sizes};
+    compress_pipeline<T, DIM, Tl>(src, smem_raw, &hdr->err);
     finish_cta(hdr, status, total_tiles);
 }
 
@@ -223,6 +232,7 @@ decompress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __r
 struct Variant {
     int warps, bpw1, bpwn;   // warps per CTA; data blocks per warp in 1D and in 2D/3D
     const void* (*kernel)(int type, int dim, bool comp);
+    size_t (*smem)(int type, int dim);   // dynamic shared memory of the compress kernel
 };
 
 template <int DIM, int WARPS, int BPW>
@@ -233,6 +243,22 @@ static const void* kernel_for_variant(int type, bool comp)
     return comp ? (const void*)compress_batch_kernel<double, DIM, Tl> : (const void*)decompress_batch_kernel<double, DIM, Tl>;
 }
 
+// Looks up (and on first use enables) the dynamic shared memory of a compress kernel.
+template <typename T, int DIM, typename Tl>
+static size_t smem_for_variant()
+{
+    static bool set[64] = {};   // the attribute is per device
+    constexpr size_t bytes = compress_smem_bytes<T, DIM, Tl>();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !set[dev]) {
+        cudaFuncSetAttribute((const void*)compress_batch_kernel<T, DIM, Tl>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        set[dev] = true;
+    }
+    return bytes;
+}
+
 template <int WARPS, int BPW1D, int BPWND>
 static const void* kv(int type, int dim, bool comp)
 {
@@ -241,12 +267,25 @@ static const void* kv(int type, int dim, bool comp)
     return kernel_for_variant<3, WARPS, BPWND>(type, comp);
 }
 
+template <int WARPS, int BPW1D, int BPWND>
+static size_t ks(int type, int dim)
+{
+    if (type == 0) {
+        if (dim == 1) return smem_for_variant<float, 1, Tiling<1, WARPS, BPW1D>>();
+        if (dim == 2) return smem_for_variant<float, 2, Tiling<2, WARPS, BPWND>>();
+        return smem_for_variant<float, 3, Tiling<3, WARPS, BPWND>>();
+    }
+    if (dim == 1) return smem_for_variant<double, 1, Tiling<1, WARPS, BPW1D>>();
+    if (dim == 2) return smem_for_variant<double, 2, Tiling<2, WARPS, BPWND>>();
+    return smem_for_variant<double, 3, Tiling<3, WARPS, BPWND>>();
+}
+
 // (warps per CTA, blocks per warp in 1D, blocks per warp in 2D/3D)
 static const Variant kVariants[] = {
-    {8, 16, 8, kv<8, 16, 8>},
-    {4, 16, 8, kv<4, 16, 8>},
-    {8, 8, 4, kv<8, 8, 4>},
-    {16, 8, 4, kv<16, 8, 4>},
+    {8, 16, 8, kv<8, 16, 8>, ks<8, 16, 8>},
+    {4, 16, 8, kv<4, 16, 8>, ks<4, 16, 8>},
+    {8, 8, 4, kv<8, 8, 4>, ks<8, 8, 4>},
+    {16, 8, 4, kv<16, 8, 4>, ks<16, 8, 4>},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -345,8 +384,9 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     if (p->total_tiles == 0) return cudaGetLastError() == cudaSuccess ? OK : E_CUDA;
     const Variant& v = kVariants[p->variant];
     const void* fn = v.kernel(p->type, p->dim, p->compress);
+    const size_t smem = p->compress ? v.smem(p->type, p->dim) : 0;
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.warps * 32, smem);
     if (occ < 1) occ = 1;
     const int per_sm = p->ctas_per_sm > 0 ? std::min(p->ctas_per_sm, occ) : occ;
     const uint64_t want = (uint64_t)p->sms * per_sm;
@@ -357,7 +397,7 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     WsHeader* hdr = (WsHeader*)ws;
     unsigned long long* status = (unsigned long long*)(ws + p->status_off);
     void* args[] = {(void*)&items, (void*)&map, (void*)&total, (void*)&hdr, (void*)&status, (void*)&d_sizes};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(v.warps * 32), args, 0, s) == cudaSuccess ? OK : E_CUDA;
+    return cudaLaunchKernel(fn, dim3(grid), dim3(v.warps * 32), args, smem, s) == cudaSuccess ? OK : E_CUDA;
 }
 
 extern "C" int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
@@ -442,7 +482,8 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
         if (st) return st;
         const void* fn = kVariants[v].kernel(p->type, p->dim, p->compress);
         int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].warps * 32, 0);
+        const size_t smem = p->compress ? kVariants[v].smem(p->type, p->dim) : 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].warps * 32, smem);
         for (int c = 1; c <= std::max(1, occ); c++) {
             p->ctas_per_sm = c;
             plan_launch(p, d_sizes, stream);   // warm

@@ -211,17 +211,6 @@ __device__ __forceinline__ void lorenzo_inverse(int32_t& d0, int32_t& d1, int la
 }
 
 // --------------------------------------------------------------- compress phases
-//
-// A tile is processed in three phases so that a CTA never idles on its look-back:
-//   load(t+1) is issued right after tile t's aggregate is published, so the DRAM
-//   traffic of the next tile overlaps tile t's look-back and its payload stores.
-
-template <typename T, int DIM, typename Tl>
-struct CompressIn {
-    T v0[Tl::BPW];
-    T v1[DIM == 1 ? 1 : Tl::BPW];
-    uint32_t ok0, ok1;   // 2D/3D: validity of each block's two elements (bit j)
-};
 
 template <typename T, int DIM, typename Tl>
 struct CompressWork {
@@ -231,101 +220,6 @@ struct CompressWork {
     uint32_t myoff;   // lane j < BPW: its payload offset inside the warp's range
     uint32_t wtot;
 };
-
-// Issue the coalesced loads of one tile (one element per lane per block; two in 2D/3D).
-template <typename T, int DIM, typename Tl>
-__device__ __forceinline__ void compress_load(CompressIn<T, DIM, Tl>& L, const T* __restrict__ in, const Geom& g,
-                                              int64_t tile)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * Tl::BPW;
-    if constexpr (DIM == 1) {
-#pragma unroll
-        for (int j = 0; j < Tl::BPW; j++) {
-            const uint64_t i = (b0 + j) * 32 + lane;
-            L.v0[j] = i < g.nbEle ? ld_stream(in + i) : T(0);
-        }
-    } else {
-        BlockWalk<DIM> bw(b0, g, lane);
-        uint32_t m0 = 0, m1 = 0;
-#pragma unroll
-        for (int j = 0; j < Tl::BPW; j++) {
-            bool ok0, ok1;
-            const uint64_t base = bw.elems(g, b0 + j < g.nblocks, ok0, ok1);
-            L.v0[j] = ok0 ? ld_stream(in + base + bw.o0) : T(0);
-            L.v1[j] = ok1 ? ld_stream(in + base + bw.o1) : T(0);
-            m0 |= (uint32_t)ok0 << j;
-            m1 |= (uint32_t)ok1 << j;
-            bw.advance(g);
-        }
-        L.ok0 = m0;
-        L.ok1 = m1;
-    }
-}
-
-// Quantize, predict, reduce block maxima, choose the encoding, write the rate bytes.
-template <typename T, int DIM, int MODE, typename Tl>
-__device__ __forceinline__ void compress_codes(const CompressIn<T, DIM, Tl>& L, CompressWork<T, DIM, Tl>& K, T recip,
-                                               const Geom& g, int64_t tile, uint8_t* __restrict__ cmp)
-{
-    constexpr int BPW = Tl::BPW;
-    constexpr int W = Tl::W;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
-    if constexpr (DIM == 1) {
-#pragma unroll
-        for (int j = 0; j < BPW; j++) {
-            const uint64_t i = (b0 + j) * 32 + lane;
-            const int32_t q = quantize(L.v0[j], recip);
-            int32_t p0 = 0, p1;
-            if constexpr (MODE != MODE_FIXED) predecessors<1>(q, 0, lane, p0, p1);
-            K.c0[j] = i < g.nbEle ? wsub(q, p0) : 0;
-        }
-        K.c1[0] = 0;
-    } else {
-#pragma unroll
-        for (int j = 0; j < BPW; j++) {
-            const bool ok0 = (L.ok0 >> j) & 1u, ok1 = (L.ok1 >> j) & 1u;
-            const int32_t q0 = quantize(L.v0[j], recip), q1 = quantize(L.v1[j], recip);
-            int32_t p0 = 0, p1 = 0;
-            if constexpr (MODE != MODE_FIXED) predecessors<DIM>(q0, q1, lane, p0, p1);
-            K.c0[j] = ok0 ? wsub(q0, p0) : 0;
-            K.c1[j] = ok1 ? wsub(q1, p1) : 0;
-        }
-    }
-    // rate byte per block (block maxima: signed in 1D, unsigned in 2D/3D)
-    uint32_t wtot = 0, myrb = 0, myoff = 0;
-#pragma unroll
-    for (int j = 0; j < BPW; j++) {
-        const uint32_t a0 = uabs(K.c0[j]);
-        const uint32_t a1 = DIM == 1 ? 0u : uabs(K.c1[DIM == 1 ? 0 : j]);
-        uint32_t m, m2 = 0;
-        if constexpr (DIM == 1) {
-            m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
-            if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
-        } else {
-            m = __reduce_max_sync(FULL, max(a0, a1));
-            if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
-        }
-        const int fr1 = bitlen(m);
-        uint32_t r;
-        if constexpr (MODE == MODE_OUTLIER) {
-            const int fr2 = bitlen(m2);
-            const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
-            const int cost1 = fr1 ? W + fr1 * W : 0;
-            const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
-            r = cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
-        } else {
-            r = (uint32_t)fr1;
-        }
-        if (lane == j) { myrb = r; myoff = wtot; }
-        wtot += payload_size<DIM, MODE>(r);
-    }
-    K.wtot = wtot;
-    K.myrb = myrb;
-    K.myoff = myoff;
-    if (lane < BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)myrb;
-}
 
 // Sign maps and bit-planes of the warp's blocks at their final offsets.
 template <typename T, int DIM, int MODE, typename Tl>
@@ -428,44 +322,346 @@ struct TileShared {
     LookbackShared lb;
 };
 
-// One compress step for tile `tile` (loads already in L): codes -> publish -> issue the
-// loads of tile `next` -> look-back -> pack.  `load_next` issues the next loads.
-template <typename T, int DIM, int MODE, typename Tl, typename LoadNext>
-__device__ __forceinline__ void compress_step(CompressIn<T, DIM, Tl>& L, const Geom& g, T recip, int64_t tile,
-                                              uint8_t* __restrict__ cmp, unsigned long long* __restrict__ status,
-                                              uint32_t* err, unsigned long long* total_out, TileShared<Tl::WARPS>& sh,
-                                              LoadNext&& load_next)
+// --------------------------------------------------------------- compress pipeline
+//
+// Per CTA, tiles flow through three overlapped stages:
+//   prefetch(t+1): cp.async copies of the next tile's elements into shared memory
+//                  (no registers held while they are in flight);
+//   encode(t):     quantize, predict, rate bytes, bit-plane pack into a shared staging
+//                  buffer at tile-local offsets; post the tile aggregate;
+//   flush(t-1):    resolve the previous tile's offset (its aggregate was posted one
+//                  tile earlier, so its predecessors are normally done) and write its
+//                  staged payload with coalesced 16-byte stores.
+// No stage waits on a predecessor while DRAM traffic for the CTA could be flowing.
+
+template <typename T, int DIM, typename Tl>
+struct CompressSmem {
+    static constexpr int HALVES = DIM == 1 ? 1 : 2;
+    static constexpr int IN_ELEMS = Tl::WARPS * Tl::BPW * HALVES * 32;          // one tile of input
+    static constexpr int MAXBLK = DIM == 1 ? 4 + 4 + 4 * 31 + 4 : 8 + 4 + 8 * 32;  // worst block payload
+    static constexpr int SB_BYTES = (Tl::TB * MAXBLK + 16 + 15) / 16 * 16;     // staged payload + slack
+    static constexpr size_t bytes() { return 2 * (size_t)IN_ELEMS * sizeof(T) + 2 * (size_t)SB_BYTES; }
+    T* in[2];
+    uint8_t* sb[2];
+    __device__ __forceinline__ explicit CompressSmem(unsigned char* base)
+    {
+        in[0] = reinterpret_cast<T*>(base);
+        in[1] = in[0] + IN_ELEMS;
+        sb[0] = reinterpret_cast<uint8_t*>(in[1] + IN_ELEMS);
+        sb[1] = sb[0] + SB_BYTES;
+    }
+    // this lane's element (block j, half h) inside a tile buffer
+    __device__ __forceinline__ static int slot(int warp, int j, int h, int lane)
+    {
+        return ((warp * Tl::BPW + j) * HALVES + h) * 32 + lane;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gsrc, bool ok)
 {
-    CompressWork<T, DIM, Tl> K;
-    compress_codes<T, DIM, MODE, Tl>(L, K, recip, g, tile, cmp);
-    scan_begin<Tl::WARPS>(K.wtot, sh.warp);
-    load_next(L);
-    scan_finish<Tl::WARPS>(tile, g.ntiles, status, err, total_out, g.rate_bytes, sh.warp, &sh.base, sh.lb);
-    compress_pack<T, DIM, MODE, Tl>(K, cmp + g.rate_bytes + sh.base + sh.warp[threadIdx.x >> 5]);
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    const int n = ok ? (int)sizeof(T) : 0;   // 0: zero-fill, nothing read
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(s), "l"(gsrc), "n"(sizeof(T)), "r"(n)
+                 : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Issue the asynchronous copies of this lane's elements of `tile`.  Returns the 2D/3D
+// validity bitmasks (bit j: element of block j inside the array) through ok0/ok1.
+template <typename T, int DIM, typename Tl>
+__device__ __forceinline__ void compress_prefetch(T* __restrict__ buf, const T* __restrict__ in, const Geom& g,
+                                                  int64_t tile, uint32_t& ok0m, uint32_t& ok1m)
+{
+    using SM = CompressSmem<T, DIM, Tl>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * Tl::BPW;
+    if constexpr (DIM == 1) {
+#pragma unroll
+        for (int j = 0; j < Tl::BPW; j++) {
+            const uint64_t i = (b0 + j) * 32 + lane;
+            const bool ok = i < g.nbEle;
+            cp_async_elem(buf + SM::slot(warp, j, 0, lane), ok ? in + i : in, ok);
+        }
+        ok0m = ok1m = 0;
+    } else {
+        BlockWalk<DIM> bw(b0, g, lane);
+        uint32_t m0 = 0, m1 = 0;
+#pragma unroll
+        for (int j = 0; j < Tl::BPW; j++) {
+            bool ok0, ok1;
+            const uint64_t base = bw.elems(g, b0 + j < g.nblocks, ok0, ok1);
+            cp_async_elem(buf + SM::slot(warp, j, 0, lane), ok0 ? in + base + bw.o0 : in, ok0);
+            cp_async_elem(buf + SM::slot(warp, j, 1, lane), ok1 ? in + base + bw.o1 : in, ok1);
+            m0 |= (uint32_t)ok0 << j;
+            m1 |= (uint32_t)ok1 << j;
+            bw.advance(g);
+        }
+        ok0m = m0;
+        ok1m = m1;
+    }
+}
+
+// Quantize + predict from the prefetched tile; rate bytes to the stream; per-block
+// payload offsets inside the warp's range in lane j (myrb / myoff).
+template <typename T, int DIM, int MODE, typename Tl>
+__device__ __forceinline__ void compress_codes(const T* __restrict__ buf, uint32_t ok0m, uint32_t ok1m,
+                                               CompressWork<T, DIM, Tl>& K, T recip, const Geom& g, int64_t tile,
+                                               uint8_t* __restrict__ cmp)
+{
+    using SM = CompressSmem<T, DIM, Tl>;
+    constexpr int BPW = Tl::BPW;
+    constexpr int W = Tl::W;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
+    if constexpr (DIM == 1) {
+#pragma unroll
+        for (int j = 0; j < BPW; j++) {
+            const uint64_t i = (b0 + j) * 32 + lane;
+            const int32_t q = quantize(buf[SM::slot(warp, j, 0, lane)], recip);
+            int32_t p0 = 0, p1;
+            if constexpr (MODE != MODE_FIXED) predecessors<1>(q, 0, lane, p0, p1);
+            K.c0[j] = i < g.nbEle ? wsub(q, p0) : 0;
+        }
+        K.c1[0] = 0;
+    } else {
+#pragma unroll
+        for (int j = 0; j < BPW; j++) {
+            const bool ok0 = (ok0m >> j) & 1u, ok1 = (ok1m >> j) & 1u;
+            const int32_t q0 = quantize(buf[SM::slot(warp, j, 0, lane)], recip);
+            const int32_t q1 = quantize(buf[SM::slot(warp, j, 1, lane)], recip);
+            int32_t p0 = 0, p1 = 0;
+            if constexpr (MODE != MODE_FIXED) predecessors<DIM>(q0, q1, lane, p0, p1);
+            K.c0[j] = ok0 ? wsub(q0, p0) : 0;
+            K.c1[j] = ok1 ? wsub(q1, p1) : 0;
+        }
+    }
+    uint32_t wtot = 0, myrb = 0, myoff = 0;
+#pragma unroll
+    for (int j = 0; j < BPW; j++) {
+        const uint32_t a0 = uabs(K.c0[j]);
+        const uint32_t a1 = DIM == 1 ? 0u : uabs(K.c1[DIM == 1 ? 0 : j]);
+        uint32_t m, m2 = 0;
+        if constexpr (DIM == 1) {
+            m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
+            if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
+        } else {
+            m = __reduce_max_sync(FULL, max(a0, a1));
+            if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
+        }
+        const int fr1 = bitlen(m);
+        uint32_t r;
+        if constexpr (MODE == MODE_OUTLIER) {
+            const int fr2 = bitlen(m2);
+            const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
+            const int cost1 = fr1 ? W + fr1 * W : 0;
+            const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
+            r = cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
+        } else {
+            r = (uint32_t)fr1;
+        }
+        if (lane == j) { myrb = r; myoff = wtot; }
+        wtot += payload_size<DIM, MODE>(r);
+    }
+    K.wtot = wtot;
+    K.myrb = myrb;
+    K.myoff = myoff;
+    if (lane < BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)myrb;
+}
+
+// Writes `size` staged bytes to global `dst` (any alignment) with 16-byte stores for
+// every full aligned unit and byte stores for the two ragged ends.  All threads call.
+__device__ __forceinline__ void copy_out(const uint8_t* __restrict__ sb, uint32_t size, uint8_t* __restrict__ dst)
+{
+    if (size == 0) return;
+    const uint32_t d = (uint32_t)((uintptr_t)dst & 15);
+    uint8_t* first = dst - d;
+    const uint32_t nunits = (d + size + 15) / 16;
+    for (uint32_t u = threadIdx.x; u < nunits; u += blockDim.x) {
+        const int32_t so = (int32_t)(16 * u) - (int32_t)d;   // staged offset of this unit
+        uint8_t* gp = first + 16 * u;
+        if (so >= 0 && so + 16 <= (int32_t)size) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(sb + (so & ~3));
+            const uint32_t sh = (uint32_t)(so & 3) * 8;
+            uint4 v;
+            if (sh == 0) {
+                v = make_uint4(w[0], w[1], w[2], w[3]);
+            } else {
+                const uint32_t w4 = w[4];
+                v = make_uint4(__funnelshift_r(w[0], w[1], sh), __funnelshift_r(w[1], w[2], sh),
+                               __funnelshift_r(w[2], w[3], sh), __funnelshift_r(w[3], w4, sh));
+            }
+            __stcs(reinterpret_cast<uint4*>(gp), v);
+        } else {
+#pragma unroll 1
+            for (int b = 0; b < 16; b++) {
+                const int32_t o = so + b;
+                if (o >= 0 && o < (int32_t)size) gp[b] = sb[o];
+            }
+        }
+    }
+}
+
+// Tile context: where a tile's data and stream live (constant for a single array).
+struct TileCtx {
+    const void* in;
+    uint8_t* cmp;
+    Geom g;
+    unsigned long long* status;     // this array's tile status words
+    unsigned long long* total_out;  // this array's stream length
+    int64_t local;                  // tile index inside the array
+    int mode;
+    float eb;                       // batch: bound the recip is derived from
+};
+
+template <int WARPS>
+struct PipeShared {
+    uint32_t wt[WARPS];             // warp payload totals of the tile being encoded
+    unsigned long long base;        // resolved offset of the tile being flushed
+    int64_t ticket[2];
+    uint32_t item[2];
+};
+
+// Resolve the offset of a tile whose aggregate `agg` was posted earlier (warp 0;
+// the caller's barrier publishes sp.base).
+template <int WARPS>
+__device__ __forceinline__ void resolve_prev(const TileCtx& c, unsigned long long agg, uint32_t* err,
+                                             PipeShared<WARPS>& sp)
+{
+    if ((threadIdx.x >> 5) == 0) {
+        const uint64_t excl = c.local > 0 ? warp_lookback(c.status, c.local, err) : 0;
+        if (threadIdx.x == 0) {
+            if (c.local > 0) st_release(c.status + c.local, ST_INC | ((excl + agg) & ST_VAL));
+            if ((uint64_t)c.local == c.g.ntiles - 1) *c.total_out = c.g.rate_bytes + excl + agg;
+            sp.base = excl;
+        }
+    }
+}
+
+// Encode one tile (data already prefetched into `buf`): codes, aggregate, staged pack.
+// Returns the tile aggregate (same in every thread).  Contains one barrier.
+template <typename T, int DIM, int MODE, typename Tl>
+__device__ __forceinline__ unsigned long long encode_tile(const T* __restrict__ buf, uint32_t ok0m, uint32_t ok1m,
+                                                          const TileCtx& c, T recip, uint8_t* __restrict__ sb,
+                                                          PipeShared<Tl::WARPS>& sp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CompressWork<T, DIM, Tl> K;
+    compress_codes<T, DIM, MODE, Tl>(buf, ok0m, ok1m, K, recip, c.g, c.local, c.cmp);
+    if (lane == 0) sp.wt[warp] = K.wtot;
+    __syncthreads();
+    uint32_t woff = 0;
+    unsigned long long agg = 0;
+#pragma unroll
+    for (int w = 0; w < Tl::WARPS; w++) {
+        const uint32_t t = sp.wt[w];
+        woff += w < warp ? t : 0u;
+        agg += t;
+    }
+    if (threadIdx.x == 0) st_release(c.status + c.local, (c.local == 0 ? ST_INC : ST_AGG) | agg);
+    compress_pack<T, DIM, MODE, Tl>(K, sb + woff);
+    return agg;
+}
+
+// The tile loop shared by the single-array, batched and allocation-free kernels.
+// `Src` supplies tiles: take(sp, k) (thread 0: next ticket into slot k), ctx(sp, k, c)
+// (tile context of slot k; false once tiles run out), encode(...) (encode_tile with
+// the tile's mode and bound).
+template <typename T, int DIM, typename Tl, typename Src>
+__device__ __forceinline__ void compress_pipeline(Src& src, unsigned char* smem_raw, uint32_t* err)
+{
+    CompressSmem<T, DIM, Tl> sm(smem_raw);
+    __shared__ PipeShared<Tl::WARPS> sp;
+    if (threadIdx.x == 0) {
+        src.take(sp, 0);
+        src.take(sp, 1);
+    }
+    __syncthreads();
+    TileCtx cur, nxt, prev;
+    bool has_cur = src.ctx(sp, 0, cur);
+    bool has_nxt = src.ctx(sp, 1, nxt);
+    uint32_t ok0c = 0, ok1c = 0, ok0n = 0, ok1n = 0;
+    if (has_cur) compress_prefetch<T, DIM, Tl>(sm.in[0], static_cast<const T*>(cur.in), cur.g, cur.local, ok0c, ok1c);
+    cp_async_commit();
+    __syncthreads();   // every thread has read slot 0 before the loop refills it
+    bool has_prev = false;
+    unsigned long long prev_agg = 0;
+    int prev_buf = 0;
+    for (int it = 0; has_cur; it++) {
+        const int b = it & 1;
+        if (has_nxt)
+            compress_prefetch<T, DIM, Tl>(sm.in[b ^ 1], static_cast<const T*>(nxt.in), nxt.g, nxt.local, ok0n, ok1n);
+        cp_async_commit();
+        if (threadIdx.x == 0) src.take(sp, b);
+        cp_async_wait_prev();    // this thread's copies of the current tile have landed
+        const unsigned long long agg = src.encode(sm.in[b], ok0c, ok1c, cur, sm.sb[b], sp);
+        if (has_prev) resolve_prev<Tl::WARPS>(prev, prev_agg, err, sp);
+        __syncthreads();
+        if (has_prev) copy_out(sm.sb[prev_buf], (uint32_t)prev_agg, prev.cmp + prev.g.rate_bytes + sp.base);
+        prev = cur;
+        prev_agg = agg;
+        prev_buf = b;
+        has_prev = true;
+        cur = nxt;
+        has_cur = has_nxt;
+        ok0c = ok0n;
+        ok1c = ok1n;
+        has_nxt = src.ctx(sp, b, nxt);
+    }
+    cp_async_wait_all();
+    if (has_prev) {
+        resolve_prev<Tl::WARPS>(prev, prev_agg, err, sp);
+        __syncthreads();
+        copy_out(sm.sb[prev_buf], (uint32_t)prev_agg, prev.cmp + prev.g.rate_bytes + sp.base);
+    }
+}
+
+// Tile source of one array.
+template <typename T, int DIM, int MODE, typename Tl>
+struct SingleSource {
+    const T* in;
+    uint8_t* cmp;
+    Geom g;
+    T recip;
+    WsHeader* hdr;
+    unsigned long long* status;
+    unsigned long long* total_out;
+    __device__ __forceinline__ void take(PipeShared<Tl::WARPS>& sp, int k)
+    {
+        sp.ticket[k] = (int64_t)atomicAdd(&hdr->ticket, 1u);
+    }
+    __device__ __forceinline__ bool ctx(const PipeShared<Tl::WARPS>& sp, int k, TileCtx& c) const
+    {
+        c.in = in;
+        c.cmp = cmp;
+        c.g = g;
+        c.status = status;
+        c.total_out = total_out;
+        c.local = sp.ticket[k];
+        c.mode = MODE;
+        c.eb = 0.f;
+        return (uint64_t)c.local < g.ntiles;
+    }
+    __device__ __forceinline__ unsigned long long encode(const T* buf, uint32_t ok0, uint32_t ok1, const TileCtx& c,
+                                                         uint8_t* sb, PipeShared<Tl::WARPS>& sp) const
+    {
+        return encode_tile<T, DIM, MODE, Tl>(buf, ok0, ok1, c, recip, sb, sp);
+    }
+};
+
+template <typename T, int DIM, typename Tl>
+constexpr size_t compress_smem_bytes() { return CompressSmem<T, DIM, Tl>::bytes(); }
 
 template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
 __global__ void __launch_bounds__(Tl::THREADS, 2)
 compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T recip,
                 WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
 {
-    __shared__ TileShared<Tl::WARPS> sh;
-    if (threadIdx.x == 0) sh.ticket[0] = (int64_t)atomicAdd(&hdr->ticket, 1u);
-    __syncthreads();
-    int64_t tile = sh.ticket[0];
-    CompressIn<T, DIM, Tl> L;
-    if ((uint64_t)tile < g.ntiles) compress_load<T, DIM, Tl>(L, in, g, tile);
-    for (int it = 1; (uint64_t)tile < g.ntiles; it++) {
-        // the ticket for the next tile is read after the scan's first barrier
-        if (threadIdx.x == 0) sh.ticket[it & 1] = (int64_t)atomicAdd(&hdr->ticket, 1u);
-        int64_t next = 0;
-        compress_step<T, DIM, MODE, Tl>(L, g, recip, tile, cmp, status, &hdr->err, &hdr->total, sh,
-                                        [&](CompressIn<T, DIM, Tl>& Ln) {
-                                            next = sh.ticket[it & 1];
-                                            if ((uint64_t)next < g.ntiles) compress_load<T, DIM, Tl>(Ln, in, g, next);
-                                        });
-        tile = next;
-    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SingleSource<T, DIM, MODE, Tl> src{in, cmp, g, recip, hdr, status, &hdr->total};
+    compress_pipeline<T, DIM, Tl>(src, smem_raw, &hdr->err);
     finish_cta(hdr, status, g.ntiles);
 }
 

@@ -53,13 +53,31 @@ size_t max_stream_bytes(const Problem& p)
 
 // ------------------------------------------------------------------ dispatch tables
 
+struct KernelRef {
+    const void* fn;
+    size_t smem;   // dynamic shared memory (compress: prefetch + staging buffers)
+};
+
 template <typename T, int DIM, int MODE>
-static void* ckernel() { return (void*)compress_kernel<T, DIM, MODE>; }
+static KernelRef ckernel()
+{
+    using Tl = Tiling<DIM>;
+    static bool set[64] = {};   // the attribute is per device
+    const void* fn = (const void*)compress_kernel<T, DIM, MODE, Tl>;
+    constexpr size_t bytes = compress_smem_bytes<T, DIM, Tl>();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !set[dev]) {
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        set[dev] = true;
+    }
+    return {fn, bytes};
+}
 template <typename T, int DIM, int MODE>
-static void* dkernel() { return (void*)decompress_kernel<T, DIM, MODE>; }
+static KernelRef dkernel() { return {(const void*)decompress_kernel<T, DIM, MODE>, 0}; }
 
 template <typename T, int DIM>
-static void* pick(bool comp, int mode)
+static KernelRef pick(bool comp, int mode)
 {
     if (comp) {
         switch (mode) {
@@ -75,7 +93,7 @@ static void* pick(bool comp, int mode)
     }
 }
 
-static void* kernel_for(const Problem& p, bool comp)
+static KernelRef kernel_for(const Problem& p, bool comp)
 {
     if (p.type == 0) {
         if (p.dim == 1) return pick<float, 1>(comp, p.mode);
@@ -88,7 +106,7 @@ static void* kernel_for(const Problem& p, bool comp)
 }
 
 // Persistent grid: every SM filled to the kernel's occupancy, never more CTAs than tiles.
-static int grid_for(const void* fn, uint64_t ntiles)
+static int grid_for(const KernelRef& k, uint64_t ntiles)
 {
     static std::mutex mu;
     static int sms[64] = {0};
@@ -102,11 +120,11 @@ static int grid_for(const void* fn, uint64_t ntiles)
         std::lock_guard<std::mutex> lk(mu);
         if (dev < 64 && sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
         for (int i = 0; i < ncache; i++)
-            if (cache[i].fn == fn && cache[i].dev == dev) { occ = cache[i].occ; break; }
+            if (cache[i].fn == k.fn && cache[i].dev == dev) { occ = cache[i].occ; break; }
         if (occ == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, k.smem);
             if (occ < 1) occ = 1;
-            if (ncache < 256) cache[ncache++] = Ent{fn, dev, occ};
+            if (ncache < 256) cache[ncache++] = Ent{k.fn, dev, occ};
         }
     }
     const uint64_t want = (uint64_t)(dev < 64 ? sms[dev] : 148) * (uint64_t)occ;
@@ -116,25 +134,25 @@ static int grid_for(const void* fn, uint64_t ntiles)
 static int launch(const Problem& p, bool comp, const void* a0, void* a1, double eb, void* ws, cudaStream_t s)
 {
     if (p.g.ntiles == 0) return OK;
-    void* fn = kernel_for(p, comp);
-    const int grid = grid_for(fn, p.g.ntiles);
+    const KernelRef k = kernel_for(p, comp);
+    const int grid = grid_for(k, p.g.ntiles);
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
     Geom g = p.g;
     float ebf = (float)eb, rf = 0.5f / (float)eb;
     double rd = 0.5 / eb;
+    // compress(in, cmp, g, recip, hdr, status) / decompress(out, cmp, g, eb, hdr, status)
+    const void* src = a0;
+    void* dst = a1;
     void* args[6];
-    const void* in_or_cmp = a0;
-    void* out_or_cmp = a1;
-    args[0] = &out_or_cmp;   // placeholder, reassigned below
-    args[1] = &in_or_cmp;
+    args[0] = comp ? (void*)&src : (void*)&dst;
+    args[1] = comp ? (void*)&dst : (void*)&src;
     args[2] = &g;
     if (p.type == 0) args[3] = comp ? (void*)&rf : (void*)&ebf;
     else             args[3] = comp ? (void*)&rd : (void*)&eb;
     args[4] = &hdr;
     args[5] = &status;
-    if (comp) { args[0] = &in_or_cmp; args[1] = &out_or_cmp; }
-    cudaError_t e = cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, 0, s);
+    const cudaError_t e = cudaLaunchKernel(k.fn, dim3(grid), dim3(kThreads), args, k.smem, s);
     return e == cudaSuccess ? OK : E_CUDA;
 }
 

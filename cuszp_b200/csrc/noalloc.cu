@@ -30,31 +30,18 @@ constexpr size_t kNoAllocScratchBytes = 1u << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Same tile loop as compress_kernel, on scratch at `ws`; the stream length goes to
+// Same tile pipeline as compress_kernel, on scratch at `ws`; the stream length goes to
 // *size_out, or ~0 when a bounded look-back wait gave up.
 template <typename T, int DIM, int MODE, typename Tl = Tiling<DIM>>
 __global__ void __launch_bounds__(Tl::THREADS, 2)
 compress_noalloc_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T recip, unsigned char* ws,
                         unsigned long long* __restrict__ size_out)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(ws + sizeof(WsHeader));
-    __shared__ TileShared<Tl::WARPS> sh;
-    if (threadIdx.x == 0) sh.ticket[0] = (int64_t)atomicAdd(&hdr->ticket, 1u);
-    __syncthreads();
-    int64_t tile = sh.ticket[0];
-    CompressIn<T, DIM, Tl> L;
-    if ((uint64_t)tile < g.ntiles) compress_load<T, DIM, Tl>(L, in, g, tile);
-    for (int it = 1; (uint64_t)tile < g.ntiles; it++) {
-        if (threadIdx.x == 0) sh.ticket[it & 1] = (int64_t)atomicAdd(&hdr->ticket, 1u);
-        int64_t next = 0;
-        compress_step<T, DIM, MODE, Tl>(L, g, recip, tile, cmp, status, &hdr->err, size_out, sh,
-                                        [&](CompressIn<T, DIM, Tl>& Ln) {
-                                            next = sh.ticket[it & 1];
-                                            if ((uint64_t)next < g.ntiles) compress_load<T, DIM, Tl>(Ln, in, g, next);
-                                        });
-        tile = next;
-    }
+    SingleSource<T, DIM, MODE, Tl> src{in, cmp, g, recip, hdr, status, size_out};
+    compress_pipeline<T, DIM, Tl>(src, smem_raw, &hdr->err);
     __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -71,23 +58,24 @@ compress_noalloc_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geo
 namespace {
 
 template <typename T, int DIM>
-const void* pick_noalloc(int mode)
+const void* pick_noalloc(int mode, size_t* smem)
 {
+    *smem = compress_smem_bytes<T, DIM, Tiling<DIM>>();
     if (mode == 0) return (const void*)compress_noalloc_kernel<T, DIM, 0>;
     if (mode == 1) return (const void*)compress_noalloc_kernel<T, DIM, 1>;
     return (const void*)compress_noalloc_kernel<T, DIM, 2>;
 }
 
-const void* noalloc_kernel(const Problem& p)
+const void* noalloc_kernel(const Problem& p, size_t* smem)
 {
     if (p.type == 0) {
-        if (p.dim == 1) return pick_noalloc<float, 1>(p.mode);
-        if (p.dim == 2) return pick_noalloc<float, 2>(p.mode);
-        return pick_noalloc<float, 3>(p.mode);
+        if (p.dim == 1) return pick_noalloc<float, 1>(p.mode, smem);
+        if (p.dim == 2) return pick_noalloc<float, 2>(p.mode, smem);
+        return pick_noalloc<float, 3>(p.mode, smem);
     }
-    if (p.dim == 1) return pick_noalloc<double, 1>(p.mode);
-    if (p.dim == 2) return pick_noalloc<double, 2>(p.mode);
-    return pick_noalloc<double, 3>(p.mode);
+    if (p.dim == 1) return pick_noalloc<double, 1>(p.mode, smem);
+    if (p.dim == 2) return pick_noalloc<double, 2>(p.mode, smem);
+    return pick_noalloc<double, 3>(p.mode, smem);
 }
 
 constexpr int kMaxDevices = 64;
@@ -151,9 +139,11 @@ extern "C" int cuSZp_compress_noalloc(const void* d_oriData, unsigned char* d_cm
     if ((st = device_setup(dev, &ws, &sms))) return st;
     // a previous call may have been aborted mid-way: start from zero
     if (cudaMemsetAsync(ws, 0, need, stream) != cudaSuccess) return E_CUDA;
-    const void* fn = noalloc_kernel(p);
+    size_t smem = 0;
+    const void* fn = noalloc_kernel(p, &smem);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return E_CUDA;
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem);
     if (occ < 1) occ = 1;
     const uint64_t want = (uint64_t)sms * occ;
     const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
@@ -167,5 +157,5 @@ extern "C" int cuSZp_compress_noalloc(const void* d_oriData, unsigned char* d_cm
     args[3] = type == CUSZP_TYPE_FLOAT ? (void*)&rf : (void*)&rd;
     args[4] = (void*)&ws;
     args[5] = (void*)&d_cmpSize;
-    return cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, 0, stream) == cudaSuccess ? OK : E_CUDA;
+    return cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream) == cudaSuccess ? OK : E_CUDA;
 }
