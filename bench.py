@@ -76,51 +76,108 @@ def make_input(name, device, seed_offset=0):
     return x.contiguous()
 
 
-class ClockSampler:
-    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+def gpu_uuid(device):
+    """NVML identity of a torch device (CUDA_VISIBLE_DEVICES renumbers devices, NVML
+    and nvidia-smi do not)."""
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(device).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
 
-    def __init__(self, index: int):
-        self.index = index
-        self.samples = []
+
+class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, polled every ~2 ms through NVML
+    from just before to just after the timed region (read-only queries).  Falls back
+    to `nvidia-smi -lms 100` when NVML is unavailable."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []   # (sm_mhz, max_mhz, [reason names])
+        self.stop = threading.Event()
+        self.thread = None
         self.proc = None
+        self.source = None
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+        uuid = gpu_uuid(self.device)
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByUUID(uuid) if uuid else N.nvmlDeviceGetHandleByIndex(0)
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            get_reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                N.nvmlDeviceGetCurrentClocksThrottleReasons
+            bits = [(name, getattr(N, attr, 0)) for name, attr in self.REASONS]
+
+            def poll():
+                while True:
+                    sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                    r = get_reasons(h)
+                    self.samples.append((float(sm), float(mx), [n for n, b in bits if b and r & b]))
+                    if self.stop.wait(0.002):
+                        break
+
+            self.source = "nvml"
+            self.thread = threading.Thread(target=poll, daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self._start_smi(uuid)
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 3.0:   # a sample before the region starts
+            time.sleep(0.002)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 7:
-                self.samples.append(parts)
+    def _start_smi(self, uuid):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", uuid or "0", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return
+        self.source = "nvidia-smi"
+        names = [n for n, _ in self.REASONS[:4]]
+
+        def read():
+            for line in self.proc.stdout:
+                parts = [p.strip() for p in line.split(",")]
+                try:
+                    self.samples.append((float(parts[0]), float(parts[1]),
+                                         [names[i] for i in range(4) if parts[2 + i].lower() == "active"]))
+                except (ValueError, IndexError):
+                    pass
+
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
+            time.sleep(0.15)   # one more nvidia-smi sample after the region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
 
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted({r for s in self.samples for r in s[2]}),
+                "samples": len(self.samples), "source": self.source}
 
 
 def traffic_summary():
@@ -165,8 +222,8 @@ def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
     return_clock = None
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(device.index or 0) as clk:
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
         t0.record(stream)
         for i in range(steps):
             ev[i][0].record(stream)
@@ -176,7 +233,7 @@ def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
             ev[i][2].record(stream)
         t1.record(stream)
         torch.cuda.synchronize()
-        return_clock = clk.summary()
+    return_clock = clk.summary()
     ws.check(stream)
     total_ms = t0.elapsed_time(t1)
     c_ms = [e[0].elapsed_time(e[1]) for e in ev]
@@ -255,8 +312,10 @@ def run_e2e(x, lay, eb, mode, dim, steps, warmup, S):
             "path": "pycuSZp -> cuSZp_compress/cuSZp_decompress (C ABI), pinned host buffers"}
 
 
-def cpu_baseline(name, device, sample_slices=None):
-    """The CPU oracle (C restatement, OpenMP over blocks) on a bounded sample."""
+def cpu_baseline(name, device, min_seconds=10.0, max_seconds=30.0, reps=None, warmup=1):
+    """The CPU oracle (C restatement, OpenMP over blocks) on a bounded sample of the
+    workload: round trips (compress + decompress) of the sample are repeated until
+    `min_seconds` of CPU work (or exactly `reps` of them after `warmup` untimed ones)."""
     import numpy as np
     import torch
     from cuszp_b200 import codec
@@ -265,7 +324,7 @@ def cpu_baseline(name, device, sample_slices=None):
     x = make_input(name, device)
     eb = codec.rel_error_bound(x, ebv) if ebk == "rel" else ebv
     if len(shape) == 3:
-        z = sample_slices or max(4, min(shape[0], (16 << 20) // (shape[1] * shape[2])))
+        z = max(4, min(shape[0], (16 << 20) // (shape[1] * shape[2])))
         xs = x[:z].contiguous()
         sample = f"first {z} of {shape[0]} z-slices ({xs.numel()} elements)"
     else:
@@ -277,18 +336,29 @@ def cpu_baseline(name, device, sample_slices=None):
     del x
     # parity of the GPU codec with the oracle on the sample (bit-exact stream)
     g_stream = codec.compress(xs, eb, mode, dim=dim, dims=lay.dims).cpu().numpy()
-    best = None
-    for _ in range(3):
+    m = codec.MODES[mode]
+    for _ in range(warmup):
+        s, _ = O.compress(h, eb, m, dim, lay.dims)
+        O.decompress(s, lay.n, h.dtype, eb, m, dim, lay.dims)
+    tc = td = 0.0
+    n = 0
+    t_start = time.perf_counter()
+    while True:
         t0 = time.perf_counter()
-        s, _ = O.compress(h, eb, codec.MODES[mode], dim, lay.dims)
+        s, _ = O.compress(h, eb, m, dim, lay.dims)
         t1 = time.perf_counter()
-        O.decompress(s, lay.n, h.dtype, eb, codec.MODES[mode], dim, lay.dims)
+        O.decompress(s, lay.n, h.dtype, eb, m, dim, lay.dims)
         t2 = time.perf_counter()
-        if best is None or (t2 - t0) < best[0]:
-            best = (t2 - t0, t1 - t0, t2 - t1)
+        tc += t1 - t0
+        td += t2 - t1
+        n += 1
+        el = t2 - t_start
+        if (reps is not None and n >= reps) or (reps is None and (el >= min_seconds or el >= max_seconds)):
+            break
     nb = h.nbytes
-    return {"value": nb / best[0] / 1e9, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
-            "sample": sample, "compress_gbs": nb / best[1] / 1e9, "decompress_gbs": nb / best[2] / 1e9,
+    return {"value": nb * n / (tc + td) / 1e9, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{sample}; {n} round trips (compress + decompress), {tc + td:.1f} s of CPU work",
+            "compress_gbs": nb * n / tc / 1e9, "decompress_gbs": nb * n / td / 1e9,
             "stream_identical_to_gpu": bool(np.array_equal(g_stream, s))}
 
 
@@ -521,7 +591,7 @@ def reference_arm(args):
     import torch
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
-    base = cpu_baseline(args.workload, device)
+    base = cpu_baseline(args.workload, device, reps=args.steps, warmup=min(args.warmup, 3))
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "GB/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",

@@ -231,8 +231,11 @@ def serve_sequential(requests: list, open_loop: bool = True) -> dict:
     t0 = time.perf_counter()
     for r in sorted(requests, key=lambda r: r.arrival):
         if open_loop:
-            while time.perf_counter() - t0 < r.arrival:
-                time.sleep(min(1e-3, r.arrival - (time.perf_counter() - t0)))
+            while True:
+                left = r.arrival - (time.perf_counter() - t0)
+                if left <= 0:
+                    break
+                time.sleep(min(1e-3, left))
         r.admitted = time.perf_counter() - t0
         lay = r.layout
         t = TYPES[r.dtype]
