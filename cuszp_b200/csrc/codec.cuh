@@ -105,7 +105,11 @@ __device__ __forceinline__ void st_stream(double* p, double v) { __stcs(p, v); }
 
 // 32x32 bit-matrix transpose across a warp: on entry the lane whose row index is
 // `row` holds row `row` (bit b = M[row][b]); on exit lane p holds column p (bit r =
-// M[r][p]).  5 butterfly stages of one shuffle, one shift select and one LOP3.
+// M[r][p]).  5 butterfly stages of one shuffle, one rotate and one LOP3: in the stage
+// of distance j a lane keeps its own half of each 2j-bit group and takes the other
+// half from its partner, whose bits sit j places away -- (y >> j) for the upper
+// partner, (y << j) for the lower one, which under the stage's mask equal rotations
+// of y right by j and by 32 - j.
 // With row = lane the transpose is the plain one.  With row = lane ^ 7 the element
 // held by lane l lands on bit l ^ 7 of every column word -- the reference's byte
 // layout (8 elements per byte, first element in the most significant bit) -- so a
@@ -116,13 +120,31 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int row)
     for (int j = 16; j >= 1; j >>= 1) {
         const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
                          : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
-        uint32_t y = __shfl_xor_sync(FULL, x, j);
+        const uint32_t y = __shfl_xor_sync(FULL, x, j);
         const bool up = row & j;
         const uint32_t keep = up ? m : ~m;
-        const uint32_t sh = up ? (y >> j) : (y << j);
+        const uint32_t sh = __funnelshift_r(y, y, up ? j : 32 - j);
         x = (x & keep) | (sh & ~keep);
     }
     return x;
+}
+
+// Two independent transposes, interleaved stage by stage (twice the work per
+// dependent step of the butterfly).
+__device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, int row)
+{
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
+                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+        const uint32_t ya = __shfl_xor_sync(FULL, a, j);
+        const uint32_t yb = __shfl_xor_sync(FULL, b, j);
+        const bool up = row & j;
+        const uint32_t keep = up ? m : ~m;
+        const int rot = up ? j : 32 - j;
+        a = (a & keep) | (__funnelshift_r(ya, ya, rot) & ~keep);
+        b = (b & keep) | (__funnelshift_r(yb, yb, rot) & ~keep);
+    }
 }
 
 // Word with bit l = element l  <->  stored little-endian word whose byte b holds

@@ -131,22 +131,24 @@ __device__ __forceinline__ void predecessors(int32_t q0, int32_t q1, int lane, i
         int32_t u = __shfl_up_sync(FULL, q0, 1);
         p0 = lane ? u : 0;
         p1 = 0;
-    } else if constexpr (DIM == 2) {
-        // x-delta inside a row, column 0 against the previous row's column 0.
-        const int32_t u1a = __shfl_up_sync(FULL, q0, 1), u8a = __shfl_up_sync(FULL, q0, 8);
-        const int32_t u1b = __shfl_up_sync(FULL, q1, 1), u8b = __shfl_up_sync(FULL, q1, 8);
-        const int32_t r3 = __shfl_sync(FULL, q0, 24);
-        const bool c0 = (lane & 7) == 0;
-        p0 = !c0 ? u1a : (lane >= 8 ? u8a : 0);
-        p1 = !c0 ? u1b : (lane >= 8 ? u8b : r3);
     } else {
-        // x-delta; row start against previous row start; plane start against previous plane start.
-        const int32_t u1a = __shfl_up_sync(FULL, q0, 1), u4a = __shfl_up_sync(FULL, q0, 4), u16a = __shfl_up_sync(FULL, q0, 16);
-        const int32_t u1b = __shfl_up_sync(FULL, q1, 1), u4b = __shfl_up_sync(FULL, q1, 4), u16b = __shfl_up_sync(FULL, q1, 16);
-        const int32_t z1 = __shfl_sync(FULL, q0, 16);
-        const int xx = lane & 3, yy = (lane >> 2) & 3;
-        p0 = xx ? u1a : yy ? u4a : (lane >= 16 ? u16a : 0);
-        p1 = xx ? u1b : yy ? u4b : (lane >= 16 ? u16b : z1);
+        // Every element but the block's first has one predecessor inside its own half,
+        // at a per-lane source lane: 2D: x-delta inside a row, column 0 against the
+        // previous row's column 0; 3D: x-delta, row start against the previous row start,
+        // plane start against the previous plane start.  Lane 0 has no predecessor in
+        // half 0, and its half-1 predecessor is half 0's element at lane 24 (2D: row 3,
+        // column 0) or lane 16 (3D: plane 1 start) -- so lane 0 reads that lane in the
+        // half-0 shuffle and one shuffle per half covers the block.
+        int src;
+        if constexpr (DIM == 2) {
+            src = (lane & 7) ? lane - 1 : (lane >= 8 ? lane - 8 : 24);
+        } else {
+            src = (lane & 3) ? lane - 1 : ((lane >> 2) & 3) ? lane - 4 : (lane ^ 16);
+        }
+        const int32_t r0 = __shfl_sync(FULL, q0, src);
+        const int32_t r1 = __shfl_sync(FULL, q1, src);
+        p0 = lane ? r0 : 0;
+        p1 = lane ? r1 : r0;
     }
 }
 
@@ -221,6 +223,176 @@ struct CompressWork {
     uint32_t wtot;
 };
 
+// Rate byte of one block from its lanes' code magnitudes (a1: 2D/3D second half).
+// 1D reduces the magnitudes as signed ints (|INT_MIN| drops out, as in the reference).
+template <int DIM, int MODE>
+__device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lane)
+{
+    constexpr int W = DIM == 1 ? 4 : 8;
+    uint32_t m, m2 = 0;
+    if constexpr (DIM == 1) {
+        m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
+        if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
+    } else {
+        m = __reduce_max_sync(FULL, max(a0, a1));
+        if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
+    }
+    const int fr1 = bitlen(m);
+    if constexpr (MODE == MODE_OUTLIER) {
+        const int fr2 = bitlen(m2);
+        const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
+        const int cost1 = fr1 ? W + fr1 * W : 0;
+        const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
+        return cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
+    } else {
+        return (uint32_t)fr1;
+    }
+}
+
+// Plane-word stores.  Blocks of rate <= 15 (the common case) carry each element's
+// sign in bit 15 of its 16-bit magnitude slot, so one 32x32 transpose yields the
+// planes and, as plane 15, the sign map already in stream byte order; the lane
+// holding plane 15 stores it as the sign word.  Wider blocks transpose the
+// magnitudes and take the sign maps from ballots.
+
+// Payload of two 1D blocks A and B (rates rA, rB; codes cA, cB of this lane) at pA / pB.
+template <int MODE>
+__device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t cA, int32_t cB, uint8_t* pA,
+                                             uint8_t* pB, int lane)
+{
+    uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
+    if constexpr (MODE == MODE_OUTLIER) {
+        nA = rA & 0x1f; nB = rB & 0x1f;
+        if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
+        if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
+    }
+    uint32_t aA = uabs(cA), aB = uabs(cB);
+    if constexpr (MODE == MODE_OUTLIER) {
+        // element 0's magnitude, little-endian, one byte per lane (lanes 0-3: A, 4-7: B)
+        const uint32_t oA = __shfl_sync(FULL, aA, 0), oB = __shfl_sync(FULL, aB, 0);
+        const uint32_t i = lane & 3;
+        if (lane < 4 && i < obA) pA[i] = (uint8_t)(oA >> (8 * i));
+        if (lane >= 4 && lane < 8 && i < obB) pB[i] = (uint8_t)(oB >> (8 * i));
+        if (lane == 0) {
+            if (obA) aA = 0;
+            if (obB) aB = 0;
+        }
+        pA += obA; pB += obB;
+    }
+    const bool hasA = payload_size<1, MODE>(rA) != 0, hasB = payload_size<1, MODE>(rB) != 0;
+    if (nA <= 15 && nB <= 15) {
+        // lane l holds plane (l ^ 7) & 15 of block A (l < 16) or B (l >= 16); plane 15 = signs
+        // (masks: a |INT_MIN| code, which the 1D rate ignores, must not reach the sign bits)
+        const uint32_t x = (aA & 0x7fffu) | ((aB << 16) & 0x7fff0000u) | (((uint32_t)cA >> 16) & 0x8000u) |
+                           ((uint32_t)cB & 0x80000000u);
+        const uint32_t y = warp_transpose32(x, lane ^ 7);
+        const uint32_t p = (lane ^ 7) & 15;
+        const bool b = lane >= 16;
+        const uint32_t n = b ? nB : nA;
+        uint8_t* q = b ? pB : pA;
+        if (p == 15) {
+            if (b ? hasB : hasA) put32<MODE>(q, y);
+        } else if (p < n) {
+            put32<MODE>(q + 4 + 4 * p, y);
+        }
+    } else {
+        const uint32_t sA = to_stream_word(__ballot_sync(FULL, cA < 0));
+        const uint32_t sB = to_stream_word(__ballot_sync(FULL, cB < 0));
+        if (lane == 0 && hasA) put32<MODE>(pA, sA);
+        if (lane == 16 && hasB) put32<MODE>(pB, sB);
+        const uint32_t yA = warp_transpose32(aA, lane ^ 7);
+        const uint32_t yB = warp_transpose32(aB, lane ^ 7);
+        const int p = lane ^ 7;
+        if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, yA);
+        if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, yB);
+    }
+}
+
+// Payload of one 2D/3D block (rate r != 0; codes c0, c1 of this lane's two elements) at p.
+template <int MODE>
+__device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1, uint8_t* p, int lane)
+{
+    uint32_t n = r, ob = 0;
+    if constexpr (MODE == MODE_OUTLIER) {
+        n = r & 0x1f;
+        if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
+    }
+    uint32_t a0 = uabs(c0);
+    const uint32_t a1 = uabs(c1);
+    if constexpr (MODE == MODE_OUTLIER) {
+        // element 0's magnitude, little-endian, one byte per lane
+        const uint32_t o = __shfl_sync(FULL, a0, 0);
+        if ((uint32_t)lane < ob) p[lane] = (uint8_t)(o >> (8 * lane));
+        if (lane == 0 && ob) a0 = 0;
+        p += ob;
+    }
+    if (n <= 15) {
+        // lane l holds plane (l ^ 7) & 15 of half l >> 4; plane 15 = the half's signs
+        const uint32_t x = (a0 & 0x7fffu) | ((a1 << 16) & 0x7fff0000u) | (((uint32_t)c0 >> 16) & 0x8000u) |
+                           ((uint32_t)c1 & 0x80000000u);
+        const uint32_t y = warp_transpose32(x, lane ^ 7);
+        const uint32_t pl = (lane ^ 7) & 15;
+        const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
+        if (pl == 15) put32<MODE>(p + h4, y);
+        else if (pl < n) put32<MODE>(p + 8 + 8 * pl + h4, y);
+    } else {
+        const uint32_t s0 = to_stream_word(__ballot_sync(FULL, c0 < 0));
+        const uint32_t s1 = to_stream_word(__ballot_sync(FULL, c1 < 0));
+        if (lane < 2) put32<MODE>(p + 4 * lane, lane ? s1 : s0);
+        const uint32_t ylo = warp_transpose32(a0, lane ^ 7);
+        const uint32_t yhi = warp_transpose32(a1, lane ^ 7);
+        const int pl = lane ^ 7;
+        if ((uint32_t)pl < n) {
+            put32<MODE>(p + 8 + 8 * pl, ylo);
+            put32<MODE>(p + 12 + 8 * pl, yhi);
+        }
+    }
+}
+
+// Payloads of two 2D/3D blocks a and b (rates ra, rb, not both 0) at pa / pb; both
+// blocks' transposes run interleaved when both rates are <= 15.
+template <int MODE>
+__device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c0a, int32_t c1a, int32_t c0b,
+                                             int32_t c1b, uint8_t* pa, uint8_t* pb, int lane)
+{
+    uint32_t na = ra, nb = rb, oba = 0, obb = 0;
+    if constexpr (MODE == MODE_OUTLIER) {
+        na = ra & 0x1f; nb = rb & 0x1f;
+        if (ra & 0x80) oba = ((ra & 0x60) >> 5) + 1;
+        if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
+    }
+    if (na > 15 || nb > 15) {
+        if (ra) pack_block_nd<MODE>(ra, c0a, c1a, pa, lane);
+        if (rb) pack_block_nd<MODE>(rb, c0b, c1b, pb, lane);
+        return;
+    }
+    uint32_t a0a = uabs(c0a), a0b = uabs(c0b);
+    const uint32_t a1a = uabs(c1a), a1b = uabs(c1b);
+    if constexpr (MODE == MODE_OUTLIER) {
+        // element 0's magnitude, little-endian, one byte per lane (lanes 0-3: a, 4-7: b)
+        const uint32_t oa = __shfl_sync(FULL, a0a, 0), ob = __shfl_sync(FULL, a0b, 0);
+        const uint32_t i = lane & 3;
+        if (lane < 4 && i < oba) pa[i] = (uint8_t)(oa >> (8 * i));
+        if (lane >= 4 && lane < 8 && i < obb) pb[i] = (uint8_t)(ob >> (8 * i));
+        if (lane == 0) {
+            if (oba) a0a = 0;
+            if (obb) a0b = 0;
+        }
+        pa += oba; pb += obb;
+    }
+    // lane l holds plane (l ^ 7) & 15 of half l >> 4; plane 15 = the half's signs
+    uint32_t xa = (a0a & 0x7fffu) | ((a1a << 16) & 0x7fff0000u) | (((uint32_t)c0a >> 16) & 0x8000u) |
+                  ((uint32_t)c1a & 0x80000000u);
+    uint32_t xb = (a0b & 0x7fffu) | ((a1b << 16) & 0x7fff0000u) | (((uint32_t)c0b >> 16) & 0x8000u) |
+                  ((uint32_t)c1b & 0x80000000u);
+    warp_transpose32x2(xa, xb, lane ^ 7);
+    const uint32_t pl = (lane ^ 7) & 15;
+    const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
+    const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
+    if (ra && (pl == 15 || pl < na)) put32<MODE>(pa + o, xa);
+    if (rb && (pl == 15 || pl < nb)) put32<MODE>(pb + o, xb);
+}
+
 // Sign maps and bit-planes of the warp's blocks at their final offsets.
 template <typename T, int DIM, int MODE, typename Tl>
 __device__ __forceinline__ void compress_pack(const CompressWork<T, DIM, Tl>& K, uint8_t* __restrict__ pbase)
@@ -232,81 +404,15 @@ __device__ __forceinline__ void compress_pack(const CompressWork<T, DIM, Tl>& K,
         for (int j = 0; j < BPW; j += 2) {
             const uint32_t rA = __shfl_sync(FULL, K.myrb, j), rB = __shfl_sync(FULL, K.myrb, j + 1);
             if ((rA | rB) == 0) continue;
-            uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
-            if constexpr (MODE == MODE_OUTLIER) {
-                nA = rA & 0x1f; nB = rB & 0x1f;
-                if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
-                if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
-            }
-            uint32_t aA = uabs(K.c0[j]), aB = uabs(K.c0[j + 1]);
-            uint8_t* pA = pbase + __shfl_sync(FULL, K.myoff, j);
-            uint8_t* pB = pbase + __shfl_sync(FULL, K.myoff, j + 1);
-            if constexpr (MODE == MODE_OUTLIER) {
-                if (lane == 0) {
-                    for (uint32_t i = 0; i < obA; i++) pA[i] = (uint8_t)(aA >> (8 * i));
-                    for (uint32_t i = 0; i < obB; i++) pB[i] = (uint8_t)(aB >> (8 * i));
-                    if (obA) aA = 0;
-                    if (obB) aB = 0;
-                }
-                pA += obA; pB += obB;
-            }
-            const uint32_t sA = to_stream_word(__ballot_sync(FULL, K.c0[j] < 0));
-            const uint32_t sB = to_stream_word(__ballot_sync(FULL, K.c0[j + 1] < 0));
-            const bool hasA = payload_size<DIM, MODE>(rA) != 0, hasB = payload_size<DIM, MODE>(rB) != 0;
-            if (lane == 0 && hasA) put32<MODE>(pA, sA);
-            if (lane == 16 && hasB) put32<MODE>(pB, sB);
-            if (nA <= 16 && nB <= 16) {
-                // lane l holds plane (l ^ 7) & 15 of block A (l < 16) or B (l >= 16)
-                const uint32_t y = warp_transpose32((aA & 0xffffu) | (aB << 16), lane ^ 7);
-                const int p = (lane ^ 7) & 15;
-                if (lane < 16) { if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, y); }
-                else           { if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, y); }
-            } else {
-                const uint32_t yA = warp_transpose32(aA, lane ^ 7);
-                const uint32_t yB = warp_transpose32(aB, lane ^ 7);
-                const int p = lane ^ 7;
-                if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, yA);
-                if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, yB);
-            }
+            pack_pair_1d<MODE>(rA, rB, K.c0[j], K.c0[j + 1], pbase + __shfl_sync(FULL, K.myoff, j),
+                               pbase + __shfl_sync(FULL, K.myoff, j + 1), lane);
         }
     } else {
 #pragma unroll
         for (int j = 0; j < BPW; j++) {
             const uint32_t r = __shfl_sync(FULL, K.myrb, j);
             if (r == 0) continue;
-            uint32_t n = r, ob = 0;
-            if constexpr (MODE == MODE_OUTLIER) {
-                n = r & 0x1f;
-                if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
-            }
-            uint32_t a0 = uabs(K.c0[j]);
-            const uint32_t a1 = uabs(K.c1[DIM == 1 ? 0 : j]);
-            uint8_t* p = pbase + __shfl_sync(FULL, K.myoff, j);
-            if constexpr (MODE == MODE_OUTLIER) {
-                if (lane == 0) {
-                    for (uint32_t i = 0; i < ob; i++) p[i] = (uint8_t)(a0 >> (8 * i));
-                    if (ob) a0 = 0;
-                }
-                p += ob;
-            }
-            const uint32_t s0 = to_stream_word(__ballot_sync(FULL, K.c0[j] < 0));
-            const uint32_t s1 = to_stream_word(__ballot_sync(FULL, K.c1[DIM == 1 ? 0 : j] < 0));
-            if (lane == 0) put32<MODE>(p, s0);
-            if (lane == 1) put32<MODE>(p + 4, s1);
-            if (n <= 16) {
-                // lane l holds plane (l ^ 7) & 15 of half l >> 4
-                const uint32_t y = warp_transpose32((a0 & 0xffffu) | (a1 << 16), lane ^ 7);
-                const int pl = (lane ^ 7) & 15;
-                if ((uint32_t)pl < n) put32<MODE>(p + 8 + 8 * pl + (lane >> 4) * 4, y);
-            } else {
-                const uint32_t ylo = warp_transpose32(a0, lane ^ 7);
-                const uint32_t yhi = warp_transpose32(a1, lane ^ 7);
-                const int pl = lane ^ 7;
-                if ((uint32_t)pl < n) {
-                    put32<MODE>(p + 8 + 8 * pl, ylo);
-                    put32<MODE>(p + 12 + 8 * pl, yhi);
-                }
-            }
+            pack_block_nd<MODE>(r, K.c0[j], K.c1[DIM == 1 ? 0 : j], pbase + __shfl_sync(FULL, K.myoff, j), lane);
         }
     }
 }
@@ -413,7 +519,6 @@ __device__ __forceinline__ void compress_codes(const T* __restrict__ buf, uint32
 {
     using SM = CompressSmem<T, DIM, Tl>;
     constexpr int BPW = Tl::BPW;
-    constexpr int W = Tl::W;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t b0 = (uint64_t)tile * Tl::TB + (uint64_t)warp * BPW;
     if constexpr (DIM == 1) {
@@ -443,25 +548,7 @@ __device__ __forceinline__ void compress_codes(const T* __restrict__ buf, uint32
     for (int j = 0; j < BPW; j++) {
         const uint32_t a0 = uabs(K.c0[j]);
         const uint32_t a1 = DIM == 1 ? 0u : uabs(K.c1[DIM == 1 ? 0 : j]);
-        uint32_t m, m2 = 0;
-        if constexpr (DIM == 1) {
-            m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
-            if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
-        } else {
-            m = __reduce_max_sync(FULL, max(a0, a1));
-            if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
-        }
-        const int fr1 = bitlen(m);
-        uint32_t r;
-        if constexpr (MODE == MODE_OUTLIER) {
-            const int fr2 = bitlen(m2);
-            const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
-            const int cost1 = fr1 ? W + fr1 * W : 0;
-            const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
-            r = cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
-        } else {
-            r = (uint32_t)fr1;
-        }
+        const uint32_t r = block_rate<DIM, MODE>(a0, a1, lane);
         if (lane == j) { myrb = r; myoff = wtot; }
         wtot += payload_size<DIM, MODE>(r);
     }

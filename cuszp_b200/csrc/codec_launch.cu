@@ -3,7 +3,10 @@
 // value-range reduction used for relative error bounds.
 #include "codec_launch.cuh"
 #include "codec_kernels.cuh"
+#include "compress_tma.cuh"
 
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 namespace cuszp {
@@ -131,9 +134,139 @@ static int grid_for(const KernelRef& k, uint64_t ntiles)
     return (int)(ntiles < want ? ntiles : want);
 }
 
+// ------------------------------------------------------------------ TMA compress path
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, looked up once through the runtime (no libcuda link).
+static EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+// 2D/3D: the array as a 3D tensor (x fastest) with one data block per box.
+static bool make_block_map(CUtensorMap* m, const Problem& p, const void* in)
+{
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t esz = p.type == 0 ? 4 : 8;
+    const cuuint64_t dims[3] = {p.g.dx, p.g.dy, p.g.dz};
+    const cuuint64_t strides[2] = {p.g.dx * esz, (cuuint64_t)p.g.dx * p.g.dy * esz};
+    const cuuint32_t box[3] = {p.dim == 2 ? 8u : 4u, p.dim == 2 ? 8u : 4u, p.dim == 2 ? 1u : 4u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, p.type == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+               const_cast<void*>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, int DIM, int MODE>
+static KernelRef tma_kernel()
+{
+    static bool set[64] = {};   // the attribute is per device
+    const void* fn = (const void*)compress_tma_kernel<T, DIM, MODE>;
+    constexpr size_t bytes = TmaCfg<T, DIM>::smem_bytes();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !set[dev]) {
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        set[dev] = true;
+    }
+    return {fn, bytes};
+}
+
+template <typename T, int DIM>
+static KernelRef tma_pick(int mode)
+{
+    switch (mode) {
+        case 0: return tma_kernel<T, DIM, 0>();
+        case 1: return tma_kernel<T, DIM, 1>();
+        default: return tma_kernel<T, DIM, 2>();
+    }
+}
+
+static KernelRef tma_kernel_for(const Problem& p)
+{
+    if (p.type == 0) {
+        if (p.dim == 1) return tma_pick<float, 1>(p.mode);
+        if (p.dim == 2) return tma_pick<float, 2>(p.mode);
+        return tma_pick<float, 3>(p.mode);
+    }
+    if (p.dim == 1) return tma_pick<double, 1>(p.mode);
+    if (p.dim == 2) return tma_pick<double, 2>(p.mode);
+    return tma_pick<double, 3>(p.mode);
+}
+
+// CUSZP_NO_TMA=1 in the environment selects the cp.async compress kernels for every input.
+static bool tma_allowed()
+{
+    static const bool ok = [] {
+        const char* e = std::getenv("CUSZP_NO_TMA");
+        return !(e && e[0] == '1');
+    }();
+    return ok;
+}
+
+// Compress through the TMA kernel when the input starts on a 16-byte boundary (and the
+// tensor map encodes); returns -1 when the caller should use the cp.async kernel.
+static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, void* ws, cudaStream_t s)
+{
+    if (!tma_allowed() || (reinterpret_cast<uintptr_t>(in) & 15u)) return -1;
+    alignas(64) CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    if (p.dim != 1 && !make_block_map(&map, p, in)) return -1;
+    const KernelRef k = tma_kernel_for(p);
+    static std::mutex mu;
+    static int sms[64] = {0};
+    static int occ_cache[64][2][3][3] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return -1;
+    int occ = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        int& c = occ_cache[dev][p.type][p.dim - 1][p.mode];
+        if (c == 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, p.type == 0 ? TmaCfg<float, 1>::THREADS
+                                                                                : TmaCfg<double, 1>::THREADS,
+                                                          k.smem);
+            if (c < 1) c = 1;
+        }
+        occ = c;
+    }
+    const uint64_t want = (uint64_t)sms[dev] * (uint64_t)occ;
+    const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
+    WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
+    Geom g = p.g;
+    float rf = 0.5f / (float)eb;
+    double rd = 0.5 / eb;
+    const void* src = in;
+    void* dst = cmp;
+    void* args[] = {(void*)&map, (void*)&src, (void*)&dst, (void*)&g, p.type == 0 ? (void*)&rf : (void*)&rd,
+                    (void*)&hdr, (void*)&status};
+    const unsigned threads = TmaCfg<float, 1>::THREADS;
+    return cudaLaunchKernel(k.fn, dim3(grid), dim3(threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
+}
+
 static int launch(const Problem& p, bool comp, const void* a0, void* a1, double eb, void* ws, cudaStream_t s)
 {
     if (p.g.ntiles == 0) return OK;
+    if (comp) {
+        const int st = launch_tma(p, a0, a1, eb, ws, s);
+        if (st >= 0) return st;
+    }
     const KernelRef k = kernel_for(p, comp);
     const int grid = grid_for(k, p.g.ntiles);
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);

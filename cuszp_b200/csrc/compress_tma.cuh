@@ -1,0 +1,529 @@
+// compress_tma.cuh -- warp-specialised compress kernel for inputs that start on a
+// 16-byte boundary (every torch allocation and every cudaMalloc'd buffer).
+//
+// One CTA = 8 codec warps + 1 loader warp + RESOLVERS resolver warps.  Tiles are the
+// same as the other compress kernels' (128 blocks in 1D, 64 in 2D/3D), so the
+// workspace and stream are identical.  A tile goes through two passes, DEFER tiles
+// apart, so that its size is known -- and posted for the other CTAs' look-backs --
+// as soon as its data lands, while the bytes follow once its offset is known:
+//
+//   loader warp: takes tile tickets and loads each tile into an input slot with the
+//     Tensor Memory Accelerator -- one `cp.async.bulk` of the tile's contiguous
+//     elements in 1D, one `cp.async.bulk.tensor.3d` box per data block in 2D/3D (the
+//     box lands in the block's element order, OOB elements zero-filled) -- completing
+//     on an mbarrier.  It refills a slot as soon as the tile's rate pass is done.
+//   codec warps, rate pass (tile k): quantize + Lorenzo delta from the input slot,
+//     codes into a code slot, block rates -> rate bytes; the last warp to finish
+//     posts the tile aggregate.
+//   resolver warps: resolver r runs the decoupled look-back of the CTA's tiles
+//     k = r, r + NC, ... (those of code slot r) and publishes their offsets.
+//   codec warps, pack pass (tile k - DEFER): sign maps and bit-planes from the code
+//     slot into a warp staging region, written to the stream with 16-byte stores at
+//     the published offset.
+// Every wait is bounded; on timeout the error word records it and the kernel ends.
+#pragma once
+
+#include <cuda.h>
+
+#include "codec_kernels.cuh"
+
+namespace cuszp {
+
+template <typename T, int DIM>
+struct TmaCfg {
+    static constexpr int WARPS = 8;                           // codec warps
+    static constexpr int DEFER = 2;                           // tiles between rate and pack pass
+    static constexpr int NC = DEFER + 1;                      // code slots (4096 int32 codes each)
+    // One resolver per code slot: resolver r takes the tiles of slot r in order, so it
+    // never waits on a phase of a slot barrier whose previous phase is still open
+    // (mbarrier parity waits cannot tell a phase two ahead from one behind).
+    static constexpr int RESOLVERS = NC;
+    static constexpr int LOADER = WARPS;                      // warp index of the loader
+    static constexpr int THREADS = 32 * (WARPS + 1 + RESOLVERS);
+    static constexpr int BPW = DIM == 1 ? 16 : 8;             // data blocks per codec warp
+    static constexpr int TB = WARPS * BPW;                    // data blocks per tile
+    static constexpr int BLK = DIM == 1 ? 32 : 64;            // elements per data block
+    static constexpr int TILE_ELEMS = TB * BLK;               // 4096
+    static constexpr int TILE_BYTES = TILE_ELEMS * (int)sizeof(T);
+    static constexpr int NIN = sizeof(T) == 4 ? 2 : 1;        // input slots
+    static constexpr int MAXBLK = DIM == 1 ? 4 + 4 + 4 * 32 : 4 + 8 + 8 * 32;   // worst block payload
+    static constexpr int REGION = (BPW * MAXBLK + 4 + 15) / 16 * 16;           // + slack for word reads
+    static constexpr int OFF_IN = 0;
+    static constexpr int OFF_CODE = NIN * TILE_BYTES;
+    static constexpr int OFF_STG = OFF_CODE + NC * TILE_ELEMS * 4;
+    static constexpr int BYTES = OFF_STG + WARPS * REGION;
+    static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }   // + base alignment
+    static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
+};
+
+// ------------------------------------------------------------------ mbarrier / TMA
+
+constexpr int kWaitLimit = 1 << 22;   // bounded mbarrier waits (with back-off: seconds)
+enum : uint32_t { ERR_WAIT_TIMEOUT = 4u };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Non-blocking poll (try_wait may suspend the thread for a while before it fails).
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase with `parity` to complete; false (and the error bit set) if it
+// did not within the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint32_t* err)
+{
+    unsigned backoff = 32;
+    for (int i = 0; i < kWaitLimit; i++) {
+        if (mbar_try_wait(b, parity)) return true;
+        if ((i & 1023) == 1023 && *reinterpret_cast<volatile uint32_t*>(err)) return false;   // another wait gave up
+        __nanosleep(backoff);
+        backoff = backoff < 512 ? 2 * backoff : 512;
+    }
+    atomicOr(err, ERR_WAIT_TIMEOUT);
+    return false;
+}
+
+// One tensor box (coordinates x fastest) into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+// `bytes` (a multiple of 16) contiguous bytes from global `src` (16-byte aligned).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// ------------------------------------------------------------------ shared state
+
+template <typename T, int DIM>
+struct TmaShared {
+    using C = TmaCfg<T, DIM>;
+    uint64_t full[C::NIN];             // input slot loaded (TMA bytes + loader arrival)
+    uint64_t freed[C::NIN];            // input slot's rate pass done (one arrival per codec warp)
+    uint64_t aggd[C::NC];              // tile aggregate posted (last codec warp)
+    uint64_t based[C::NC];             // tile offset published (resolver)
+    int64_t tick[C::NIN];              // tile held by each input slot (>= ntiles: no more tiles)
+    int64_t tile_of[C::NC];            // tile held by each code slot
+    unsigned long long agg[C::NC];     // tile payload bytes
+    unsigned long long base[C::NC];    // tile payload offset (exclusive prefix)
+    uint32_t wt[C::NC][C::WARPS];      // warp payload bytes
+    uint32_t woff[C::NC][C::WARPS];    // warp offsets inside the tile
+    uint32_t cnt[C::NC];               // codec warps done with the tile's rate pass
+    int kend;                          // index in this CTA's sequence of the first missing tile
+    uint8_t rates[C::NC][C::TB];       // block rate bytes
+};
+
+// ------------------------------------------------------------------ rate pass
+
+// 1D: codes of the warp's 16 blocks of tile `t` (elements in `tin`) into `code`, their
+// rate bytes to the stream and to `rates`; returns the warp's payload bytes.
+template <typename T, int MODE>
+__device__ __forceinline__ uint32_t rate_pass_1d(const T* __restrict__ tin, int32_t* __restrict__ code,
+                                                 uint8_t* __restrict__ rates, int warp, int64_t t, const Geom& g,
+                                                 T recip, uint8_t* __restrict__ cmp, int lane)
+{
+    using C = TmaCfg<T, 1>;
+    const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
+    uint32_t off = 0, rb = 0;
+    if (b0 * 32 < g.nbEle) {
+        const T* wb = tin + warp * C::BPW * 32;
+        int32_t* wc = code + warp * C::BPW * 32;
+        const bool ragged = (b0 + C::BPW) * 32 > g.nbEle;
+#pragma unroll 2
+        for (int j = 0; j < C::BPW; j += 2) {
+            const int32_t qA = quantize(wb[j * 32 + lane], recip);
+            const int32_t qB = quantize(wb[(j + 1) * 32 + lane], recip);
+            int32_t cA = qA, cB = qB;
+            if constexpr (MODE != MODE_FIXED) {
+                const int32_t uA = __shfl_up_sync(FULL, qA, 1), uB = __shfl_up_sync(FULL, qB, 1);
+                cA = wsub(qA, lane ? uA : 0);
+                cB = wsub(qB, lane ? uB : 0);
+            }
+            if (ragged) {
+                const uint64_t i = (b0 + j) * 32 + lane;
+                cA = i < g.nbEle ? cA : 0;
+                cB = i + 32 < g.nbEle ? cB : 0;
+            }
+            wc[j * 32 + lane] = cA;
+            wc[(j + 1) * 32 + lane] = cB;
+            const uint32_t rA = block_rate<1, MODE>(uabs(cA), 0u, lane);
+            const uint32_t rB = block_rate<1, MODE>(uabs(cB), 0u, lane);
+            if (lane == j) rb = rA;
+            if (lane == j + 1) rb = rB;
+            off += payload_size<1, MODE>(rA) + payload_size<1, MODE>(rB);
+        }
+    }
+    if (lane < C::BPW) {
+        rates[warp * C::BPW + lane] = (uint8_t)rb;
+        if (b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)rb;
+    }
+    return off;
+}
+
+// 2D/3D: same for the warp's 8 blocks (each block's 64 elements contiguous in `tin`),
+// two blocks per step so that their dependency chains overlap.
+template <typename T, int DIM, int MODE>
+__device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int32_t* __restrict__ code,
+                                                 uint8_t* __restrict__ rates, int warp, int64_t t, const Geom& g,
+                                                 T recip, uint8_t* __restrict__ cmp, int lane)
+{
+    using C = TmaCfg<T, DIM>;
+    constexpr uint32_t B = DIM == 2 ? 8 : 4;
+    static_assert(C::BPW % 2 == 0, "blocks are processed in pairs");
+    const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
+    uint32_t off = 0, rbyte = 0;
+    if (b0 < g.nblocks) {
+        const T* wb = tin + warp * C::BPW * 64;
+        int32_t* wc = code + warp * C::BPW * 64;
+        const BlockPos bp = block_pos(b0, g);
+        uint32_t bx = bp.x, by = bp.y, bz = bp.z;
+        // this lane's element coordinates inside a block (halves 0 and 1)
+        const uint32_t cx = DIM == 2 ? (lane & 7) : (lane & 3);
+        const uint32_t ry0 = DIM == 2 ? (lane >> 3) : ((lane >> 2) & 3);
+        const uint32_t ry1 = DIM == 2 ? ry0 + 4 : ry0;
+        const uint32_t rz0 = DIM == 2 ? 0 : (lane >> 4);
+        const uint32_t rz1 = DIM == 2 ? 0 : rz0 + 2;
+        const uint32_t nblk = (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0);
+        // partial blocks exist only along axes the block size does not divide
+        const bool ragged = (g.dx % B) || (g.dy % B) || (DIM == 3 && (g.dz % 4));
+        auto advance = [&](uint32_t& x, uint32_t& y, uint32_t& z) {
+            if (++x == g.bxn) {
+                x = 0;
+                if (++y == g.byn) { y = 0; ++z; }
+            }
+        };
+        // codes of one block (elements outside the array: code 0)
+        auto codes = [&](const T* blk, uint32_t x, uint32_t y, uint32_t z, int32_t& c0, int32_t& c1) {
+            const int32_t q0 = quantize(blk[lane], recip);
+            const int32_t q1 = quantize(blk[32 + lane], recip);
+            c0 = q0;
+            c1 = q1;
+            if constexpr (MODE != MODE_FIXED) {
+                int32_t p0, p1;
+                predecessors<DIM>(q0, q1, lane, p0, p1);
+                c0 = wsub(q0, p0);
+                c1 = wsub(q1, p1);
+            }
+            const uint32_t xb = x * B, yb = y * B, zb = DIM == 2 ? z : z * 4;
+            if (ragged && (xb + B > g.dx || yb + B > g.dy || (DIM == 3 && zb + 4 > g.dz))) {
+                const bool inx = xb + cx < g.dx;
+                const bool ok0 = inx && yb + ry0 < g.dy && (DIM == 2 || zb + rz0 < g.dz);
+                const bool ok1 = inx && yb + ry1 < g.dy && (DIM == 2 || zb + rz1 < g.dz);
+                c0 = ok0 ? c0 : 0;
+                c1 = ok1 ? c1 : 0;
+            }
+        };
+#pragma unroll 1
+        for (uint32_t j = 0; j < nblk; j += 2) {
+            uint32_t xb2 = bx, yb2 = by, zb2 = bz;
+            advance(xb2, yb2, zb2);
+            int32_t c0a, c1a, c0b, c1b;
+            codes(wb + j * 64, bx, by, bz, c0a, c1a);
+            codes(wb + (j + 1) * 64, xb2, yb2, zb2, c0b, c1b);   // inside the warp's 8 blocks
+            if (j + 1 >= nblk) { c0b = 0; c1b = 0; }             // past the last block: rate 0
+            int32_t* ca = wc + j * 64;
+            ca[lane] = c0a;
+            ca[32 + lane] = c1a;
+            ca[64 + lane] = c0b;
+            ca[96 + lane] = c1b;
+            const uint32_t ra = block_rate<DIM, MODE>(uabs(c0a), uabs(c1a), lane);
+            const uint32_t rb = block_rate<DIM, MODE>(uabs(c0b), uabs(c1b), lane);
+            if (lane == (int)j) rbyte = ra;
+            if (lane == (int)j + 1) rbyte = rb;
+            off += payload_size<DIM, MODE>(ra) + payload_size<DIM, MODE>(rb);
+            bx = xb2; by = yb2; bz = zb2;
+            advance(bx, by, bz);
+        }
+    }
+    if (lane < C::BPW) {
+        rates[warp * C::BPW + lane] = (uint8_t)rbyte;
+        if (b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)rbyte;
+    }
+    return off;
+}
+
+// ------------------------------------------------------------------ pack pass
+
+// Sign maps and bit-planes of the warp's blocks (codes in `code`, rate bytes in
+// `rates`) into `region`; returns the payload bytes written there.
+template <int DIM, int MODE, typename C>
+__device__ __forceinline__ uint32_t pack_pass(const int32_t* __restrict__ code, const uint8_t* __restrict__ rates,
+                                              int warp, uint8_t* __restrict__ region, int lane)
+{
+    const int32_t* wc = code + warp * C::BPW * C::BLK;
+    const uint32_t mine = lane < C::BPW ? rates[warp * C::BPW + lane] : 0u;
+    uint32_t off = 0;
+#pragma unroll 1
+    for (int j = 0; j < C::BPW; j += 2) {
+        const uint32_t ra = __shfl_sync(FULL, mine, j), rb = __shfl_sync(FULL, mine, j + 1);
+        const uint32_t sa = payload_size<DIM, MODE>(ra);
+        if (ra | rb) {
+            if constexpr (DIM == 1) {
+                pack_pair_1d<MODE>(ra, rb, wc[j * 32 + lane], wc[(j + 1) * 32 + lane], region + off, region + off + sa,
+                                   lane);
+            } else {
+                const int32_t* ca = wc + j * 64;
+                pack_pair_nd<MODE>(ra, rb, ca[lane], ca[32 + lane], ca[64 + lane], ca[96 + lane], region + off,
+                                   region + off + sa, lane);
+            }
+        }
+        off += sa + payload_size<DIM, MODE>(rb);
+    }
+    return off;
+}
+
+// Warp-cooperative write of `n` staged bytes (`src` 16-byte aligned in shared memory)
+// to global `dst` (any alignment): 16-byte stores for the aligned units inside the
+// range, one byte store per lane for the ragged first and last units.
+__device__ __forceinline__ void warp_copy_out(const uint8_t* __restrict__ src, uint32_t n, uint8_t* __restrict__ dst,
+                                              int lane)
+{
+    if (n == 0) return;
+    const uint32_t d = (uint32_t)((uintptr_t)dst & 15);
+    uint8_t* first = dst - d;
+    const uint32_t u0 = d ? 1u : 0u;          // first unit entirely inside [d, d + n)
+    const uint32_t u1 = (d + n) >> 4;         // one past the last such unit
+    for (uint32_t u = u0 + lane; u < u1; u += 32) {
+        const uint32_t so = 16 * u - d;
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(src + (so & ~3u));
+        const uint32_t sh = (so & 3u) * 8;
+        uint4 v;
+        if (sh == 0) {
+            v = make_uint4(w[0], w[1], w[2], w[3]);
+        } else {
+            const uint32_t w4 = w[4];
+            v = make_uint4(__funnelshift_r(w[0], w[1], sh), __funnelshift_r(w[1], w[2], sh),
+                           __funnelshift_r(w[2], w[3], sh), __funnelshift_r(w[3], w4, sh));
+        }
+        __stcs(reinterpret_cast<uint4*>(first + 16 * u), v);
+    }
+    // ragged units: unit 0 when d != 0 (lanes 0-15), unit u1 when the range ends inside
+    // it and it is not unit 0 again (lanes 16-31)
+    const bool head = d != 0;
+    const bool tail = ((d + n) & 15u) != 0 && !(head && u1 == 0);
+    const uint32_t unit = lane < 16 ? 0u : u1;
+    if ((lane < 16 && head) || (lane >= 16 && tail)) {
+        const uint32_t pos = 16 * unit + (uint32_t)(lane & 15);
+        if (pos >= d && pos < d + n) first[pos] = src[pos - d];
+    }
+}
+
+// ------------------------------------------------------------------ the kernel
+
+template <typename T, int DIM, int MODE>
+__global__ void __launch_bounds__(TmaCfg<T, DIM>::THREADS, 2)
+compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ in, uint8_t* __restrict__ cmp,
+                    Geom g, T recip, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+{
+    using C = TmaCfg<T, DIM>;
+    extern __shared__ unsigned char dsm[];
+    unsigned char* base = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
+    T* inbuf = reinterpret_cast<T*>(base + C::OFF_IN);
+    int32_t* codebuf = reinterpret_cast<int32_t*>(base + C::OFF_CODE);
+    uint8_t* stg = base + C::OFF_STG;
+    __shared__ __align__(8) TmaShared<T, DIM> sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* err = &hdr->err;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < C::NIN; i++) {
+            mbar_init(&sh.full[i], 1);
+            mbar_init(&sh.freed[i], C::WARPS);
+        }
+        for (int i = 0; i < C::NC; i++) {
+            mbar_init(&sh.aggd[i], 1);
+            mbar_init(&sh.based[i], 1);
+            sh.cnt[i] = 0;
+        }
+        sh.kend = 0x7fffffff;
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    if (warp > C::LOADER) {
+        // ---------------------------------------------------------------- resolver warps
+        for (int k = warp - C::LOADER - 1;; k += C::RESOLVERS) {
+            const int c = k % C::NC;
+            const uint32_t parity = (uint32_t)(k / C::NC) & 1u;
+            bool ready = false;
+            unsigned backoff = 32;
+            for (int i = 0; i < kWaitLimit; i++) {   // tile k's rate pass done, or no tile k
+                if (mbar_try_wait(&sh.aggd[c], parity)) { ready = true; break; }
+                if (k >= *reinterpret_cast<volatile int*>(&sh.kend)) break;
+                if ((i & 1023) == 1023 && *reinterpret_cast<volatile uint32_t*>(err)) break;
+                __nanosleep(backoff);
+                backoff = backoff < 512 ? 2 * backoff : 512;
+            }
+            if (!ready) break;
+            const int64_t t = sh.tile_of[c];
+            const unsigned long long agg = sh.agg[c];
+            const uint64_t excl = t > 0 ? warp_lookback(status, t, err) : 0;
+            if (lane == 0) {
+                if (t > 0) st_release(status + t, ST_INC | ((excl + agg) & ST_VAL));
+                if ((uint64_t)t == g.ntiles - 1) hdr->total = g.rate_bytes + excl + agg;
+                sh.base[c] = excl;
+                mbar_arrive(&sh.based[c]);
+            }
+        }
+    } else if (warp == C::LOADER) {
+        // ---------------------------------------------------------------- loader warp
+        bool ended = false;
+        int issued = 0;   // issue() calls so far; slots are used round-robin
+        // Takes a ticket for input slot s and starts its load.  Returns false once the
+        // tickets ran past the last tile (the slot then completes with no bytes).
+        auto issue = [&](int s) -> bool {
+            int64_t t = 0;
+            issued++;
+            if (lane == 0) t = (int64_t)atomicAdd(&hdr->ticket, 1u);
+            t = __shfl_sync(FULL, t, 0);
+            T* dst = inbuf + s * C::TILE_ELEMS;
+            if ((uint64_t)t >= g.ntiles) {
+                if (lane == 0) {
+                    sh.tick[s] = t;
+                    *reinterpret_cast<volatile int*>(&sh.kend) = issued - 1;   // issue order = tile order
+                    mbar_arrive(&sh.full[s]);
+                }
+                return false;
+            }
+            if constexpr (DIM == 1) {
+                const uint64_t e0 = (uint64_t)t * C::TILE_ELEMS;
+                const uint64_t cnt = e0 < g.nbEle ? min((uint64_t)C::TILE_ELEMS, g.nbEle - e0) : 0;
+                const uint32_t bytes = (uint32_t)cnt * (uint32_t)sizeof(T);
+                const uint32_t main = bytes & ~15u;
+                const uint32_t tail = (bytes - main) / (uint32_t)sizeof(T);   // < 16 bytes of elements
+                if ((uint32_t)lane < tail) dst[main / sizeof(T) + lane] = in[e0 + main / sizeof(T) + lane];
+                __syncwarp();
+                if (lane == 0) {
+                    sh.tick[s] = t;
+                    mbar_arrive_tx(&sh.full[s], main);
+                    if (main) bulk_load(dst, in + e0, main, &sh.full[s]);
+                }
+            } else {
+                const uint64_t b0 = (uint64_t)t * C::TB;
+                const uint32_t nvalid = (uint32_t)min((uint64_t)C::TB, g.nblocks - b0);
+                if (lane == 0) {
+                    sh.tick[s] = t;
+                    mbar_arrive_tx(&sh.full[s], nvalid * 64u * (uint32_t)sizeof(T));
+                }
+                __syncwarp();
+                for (uint32_t j = lane; j < nvalid; j += 32) {
+                    const BlockPos p = block_pos(b0 + j, g);
+                    if constexpr (DIM == 2)
+                        tma_load_3d(dst + j * 64, &tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, &sh.full[s]);
+                    else
+                        tma_load_3d(dst + j * 64, &tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), &sh.full[s]);
+                }
+            }
+            return true;
+        };
+        for (int s = 0; s < C::NIN && !ended; s++) ended = !issue(s);
+        for (int k = 0;; k++) {
+            const int s = k % C::NIN;
+            __syncwarp();
+            const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tick[s]);
+            if ((uint64_t)t >= g.ntiles) break;
+            if (!mbar_wait(&sh.freed[s], (uint32_t)(k / C::NIN) & 1u, err)) break;
+            if (!ended) ended = !issue(s);   // tile k's elements are consumed: load tile k + NIN
+        }
+        // no load may still be writing shared memory when the CTA ends (only reachable
+        // with loads outstanding after a timed-out wait)
+        if (lane == 0) {
+            for (int s = 0; s < C::NIN; s++) {
+                const int uses = issued / C::NIN + (s < issued % C::NIN ? 1 : 0);
+                if (uses) mbar_wait(&sh.full[s], (uint32_t)(uses - 1) & 1u, err);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------------- codec warps
+        uint8_t* region = stg + warp * C::REGION;
+        auto pack_out = [&](int kk) -> bool {
+            const int c = kk % C::NC;
+            if (!mbar_wait(&sh.based[c], (uint32_t)(kk / C::NC) & 1u, err)) return false;
+            const uint32_t n = pack_pass<DIM, MODE, C>(codebuf + c * C::TILE_ELEMS, sh.rates[c], warp, region, lane);
+            __syncwarp();
+            warp_copy_out(region, n, cmp + g.rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
+            __syncwarp();
+            return true;
+        };
+        int k = 0;
+        for (;; k++) {
+            const int s = k % C::NIN, c = k % C::NC;
+            if (!mbar_wait(&sh.full[s], (uint32_t)(k / C::NIN) & 1u, err)) break;
+            const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tick[s]);
+            if ((uint64_t)t >= g.ntiles) break;
+            const T* tin = inbuf + s * C::TILE_ELEMS;
+            int32_t* code = codebuf + c * C::TILE_ELEMS;
+            uint32_t total;
+            if constexpr (DIM == 1)
+                total = rate_pass_1d<T, MODE>(tin, code, sh.rates[c], warp, t, g, recip, cmp, lane);
+            else
+                total = rate_pass_nd<T, DIM, MODE>(tin, code, sh.rates[c], warp, t, g, recip, cmp, lane);
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&sh.freed[s]);   // this warp is done with the input slot
+                sh.wt[c][warp] = total;
+                __threadfence_block();
+                if (atomicAdd(&sh.cnt[c], 1u) == C::WARPS - 1) {   // last warp of the tile
+                    __threadfence_block();
+                    uint32_t acc = 0;
+                    for (int w = 0; w < C::WARPS; w++) {
+                        const uint32_t x = *reinterpret_cast<volatile uint32_t*>(&sh.wt[c][w]);
+                        sh.woff[c][w] = acc;
+                        acc += x;
+                    }
+                    sh.agg[c] = acc;
+                    sh.tile_of[c] = t;
+                    sh.cnt[c] = 0;
+                    st_release(status + t, (t == 0 ? ST_INC : ST_AGG) | acc);
+                    mbar_arrive(&sh.aggd[c]);
+                }
+            }
+            if (k >= C::DEFER && !pack_out(k - C::DEFER)) break;
+        }
+        for (int kk = k - C::DEFER < 0 ? 0 : k - C::DEFER; kk < k; kk++)
+            if (!pack_out(kk)) break;
+    }
+    finish_cta(hdr, status, g.ntiles);
+}
+
+}  // namespace cuszp

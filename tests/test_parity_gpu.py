@@ -126,6 +126,57 @@ def test_matches_oracle(dtype, mode, dim, dims, n, kind):
     assert np.array_equal(got.view(np.uint8), exp.view(np.uint8))
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["fixed", "plain", "outlier"])
+@pytest.mark.parametrize("dim,dims", [(1, (0, 0, 0)), (2, (64, 40, 3)), (3, (32, 24, 20))], ids=["1d", "2d", "3d"])
+def test_block_rates_around_16_bits(dtype, mode, dim, dims):
+    """Blocks whose largest code needs 13..18 bits, signs mixed, and |code| = 2^31:
+    the packers switch between one shared and two separate bit transposes at 15/16."""
+    rng = np.random.default_rng(40 + dim)
+    n = 96 * 1024 if dim == 1 else dims[0] * dims[1] * dims[2]
+    x = rng.integers(-3, 4, n).astype(np.float64)
+    spikes = rng.integers(0, n, n // 40)
+    bits = rng.integers(13, 19, spikes.size)
+    x[spikes] = (2.0 ** bits - 1) * rng.choice([-1.0, 1.0], spikes.size)
+    x[rng.integers(0, n, 8)] = 3e9           # quantizes to the int32 limit
+    x = x.astype(dtype)
+    eb = 0.5
+    want, _ = O.compress(x, eb, mode, dim, dims)
+    buf, size = ref_compress(x, eb, mode, dim, dims)
+    assert size == want.size and np.array_equal(buf[:size], want)
+
+
+MISALIGNED_SHAPES = [(1, (0, 0, 0), 100_003), (2, (516, 301, 2), None), (3, (68, 37, 29), None)]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["fixed", "plain", "outlier"])
+@pytest.mark.parametrize("dim,dims,n", MISALIGNED_SHAPES, ids=lambda v: str(v))
+def test_input_off_16_byte_boundary_matches_oracle(dtype, mode, dim, dims, n):
+    """Inputs that do not start on a 16-byte boundary (an element-offset view) take the
+    per-element cp.async compress kernel instead of the TMA one: same bytes."""
+    from cuszp_b200 import codec
+    rng = np.random.default_rng(dim * 10 + mode)
+    if n is None:
+        n = dims[0] * dims[1] * dims[2]
+    x = _field(rng, n, "sparse").astype(dtype)
+    eb = 1e-3
+    want, _ = O.compress(x, eb, mode, dim, dims)
+    base = torch.zeros(n + 1, dtype=TT[dtype], device="cuda")
+    base[1:] = torch.from_numpy(x).cuda()
+    view = base[1:]
+    assert view.data_ptr() % 16 != 0
+    cap = O.max_stream_bytes(n, dim, dims) + 64
+    out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    size = torch.zeros(1, dtype=torch.int64, device="cuda")
+    lay = codec.Layout(n, dim, dims)
+    codec.compress_into(view, out, eb, mode, dim, lay.dims, size_out=size)
+    torch.cuda.synchronize()
+    S = int(size.item())
+    assert S == want.size
+    assert np.array_equal(out[:S].cpu().numpy(), want)
+
+
 # --------------------------------------------------------------------------- edge cases
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
