@@ -4,6 +4,7 @@
 #include "codec_launch.cuh"
 #include "codec_kernels.cuh"
 #include "compress_tma.cuh"
+#include "decompress_tma.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -260,11 +261,88 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
 }
 
+template <typename T, int DIM, int MODE>
+static KernelRef dtma_kernel()
+{
+    static bool set[64] = {};   // the attribute is per device
+    const void* fn = (const void*)decompress_tma_kernel<T, DIM, MODE>;
+    constexpr size_t bytes = DecCfg<T, DIM>::smem_bytes();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !set[dev]) {
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        set[dev] = true;
+    }
+    return {fn, bytes};
+}
+
+template <typename T, int DIM>
+static KernelRef dtma_pick(int mode)
+{
+    switch (mode) {
+        case 0: return dtma_kernel<T, DIM, 0>();
+        case 1: return dtma_kernel<T, DIM, 1>();
+        default: return dtma_kernel<T, DIM, 2>();
+    }
+}
+
+static KernelRef dtma_kernel_for(const Problem& p)
+{
+    if (p.type == 0) {
+        if (p.dim == 1) return dtma_pick<float, 1>(p.mode);
+        if (p.dim == 2) return dtma_pick<float, 2>(p.mode);
+        return dtma_pick<float, 3>(p.mode);
+    }
+    if (p.dim == 1) return dtma_pick<double, 1>(p.mode);
+    if (p.dim == 2) return dtma_pick<double, 2>(p.mode);
+    return dtma_pick<double, 3>(p.mode);
+}
+
+// Decompress through the TMA kernel when the stream and the output start on 16-byte
+// boundaries; returns -1 when the caller should use the other decompress kernel.
+static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, void* ws, cudaStream_t s)
+{
+    if (!tma_allowed() || ((reinterpret_cast<uintptr_t>(cmp) | reinterpret_cast<uintptr_t>(out)) & 15u)) return -1;
+    alignas(64) CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    if (p.dim != 1 && !make_block_map(&map, p, out)) return -1;
+    const KernelRef k = dtma_kernel_for(p);
+    static std::mutex mu;
+    static int sms[64] = {0};
+    static int occ_cache[64][2][3][3] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return -1;
+    const unsigned threads = DecCfg<float, 1>::THREADS;
+    int occ = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        int& c = occ_cache[dev][p.type][p.dim - 1][p.mode];
+        if (c == 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, threads, k.smem);
+            if (c < 1) c = 1;
+        }
+        occ = c;
+    }
+    const uint64_t want = (uint64_t)sms[dev] * (uint64_t)occ;
+    const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
+    WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
+    Geom g = p.g;
+    float ebf = (float)eb;
+    void* dst = out;
+    const void* src = cmp;
+    void* args[] = {(void*)&map, (void*)&dst, (void*)&src, (void*)&g, p.type == 0 ? (void*)&ebf : (void*)&eb,
+                    (void*)&hdr, (void*)&status};
+    return cudaLaunchKernel(k.fn, dim3(grid), dim3(threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
+}
+
 static int launch(const Problem& p, bool comp, const void* a0, void* a1, double eb, void* ws, cudaStream_t s)
 {
     if (p.g.ntiles == 0) return OK;
-    if (comp) {
-        const int st = launch_tma(p, a0, a1, eb, ws, s);
+    {
+        const int st = comp ? launch_tma(p, a0, a1, eb, ws, s) : launch_dtma(p, a0, a1, eb, ws, s);
         if (st >= 0) return st;
     }
     const KernelRef k = kernel_for(p, comp);

@@ -1,0 +1,359 @@
+// decompress_tma.cuh -- warp-specialised decompress kernel for streams and outputs that
+// start on a 16-byte boundary.
+//
+// One CTA = 8 codec warps + FRONT front warps.  Same tiles as the compress kernels.
+//
+//   front warp f owns payload slot f.  Per tile it takes a ticket, reads the tile's
+//     rate bytes, posts the tile aggregate at once (payload sizes follow from the rate
+//     bytes alone, so no tile ever waits on a predecessor that is itself waiting),
+//     runs the decoupled look-back, and loads the tile's payload bytes with one
+//     `cp.async.bulk` into its slot.  When the codec warps have decoded the slot it
+//     takes the next ticket.
+//   codec warps: take the slots round-robin; each decodes its blocks from shared
+//     memory (sign map and bit-planes -> inverse transpose -> signs -> inverse Lorenzo
+//     -> dequantize) into its own output buffer and writes them with TMA stores: one
+//     `cp.async.bulk.tensor.3d` box per 2D/3D block (elements outside the array are
+//     not written), or one `cp.async.bulk` of the warp's contiguous 1D elements.
+// Every wait is bounded; on timeout the error word records it and the kernel ends.
+#pragma once
+
+#include "compress_tma.cuh"
+
+namespace cuszp {
+
+template <typename T, int DIM>
+struct DecCfg {
+    static constexpr int WARPS = 8;                           // codec warps
+    static constexpr int FRONT = 4;                           // front warps = payload slots
+    static constexpr int THREADS = 32 * (WARPS + FRONT);
+    static constexpr int BPW = DIM == 1 ? 16 : 8;             // data blocks per codec warp
+    static constexpr int TB = WARPS * BPW;                    // data blocks per tile
+    static constexpr int BLK = DIM == 1 ? 32 : 64;            // elements per data block
+    static constexpr int MAXBLK = DIM == 1 ? 4 + 4 + 4 * 32 : 4 + 8 + 8 * 32;   // worst block payload
+    // a tile's payload plus the 16-byte rounding at both ends and word-read slack
+    static constexpr int SLOT = (TB * MAXBLK + 48 + 127) / 128 * 128;
+    static constexpr int OUTW = BPW * BLK * (int)sizeof(T);   // a codec warp's decoded elements
+    static constexpr int OFF_SLOT = 0;
+    static constexpr int OFF_OUT = FRONT * SLOT;
+    static constexpr int BYTES = OFF_OUT + WARPS * OUTW;
+    static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }
+    static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
+    static_assert(FRONT <= 8, "slot parities are kept in one byte");
+};
+
+constexpr uint32_t kBadSlot = 0xffffffffu;   // poff of a tile whose rate bytes are invalid
+
+template <typename T, int DIM>
+struct DecShared {
+    using C = DecCfg<T, DIM>;
+    uint64_t full[C::FRONT];           // slot filled (payload bytes + front arrival)
+    uint64_t freed[C::FRONT];          // slot decoded (one arrival per codec warp)
+    int64_t tile[C::FRONT];            // tile in each slot (>= ntiles: the front warp has ended)
+    uint32_t poff[C::FRONT];           // payload start inside the slot
+    uint32_t woff[C::FRONT][C::WARPS]; // codec warp offsets inside the tile payload
+    uint8_t rates[C::FRONT][C::TB];    // block rate bytes
+};
+
+// ------------------------------------------------------------------ payload words
+
+// Word at byte offset `o` of shared memory `p` (any alignment in outlier mode; the
+// payload of fixed/plain streams sits at 4-byte offsets).
+template <int MODE>
+__device__ __forceinline__ uint32_t lds32(const uint8_t* p, uint32_t o)
+{
+    if constexpr (MODE == MODE_OUTLIER) {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(p + (o & ~3u));
+        const uint32_t sh = (o & 3u) * 8;
+        return sh ? __funnelshift_r(w[0], w[1], sh) : w[0];
+    } else {
+        return *reinterpret_cast<const uint32_t*>(p + o);
+    }
+}
+// Element 0's magnitude stored in `ob` little-endian bytes at offset `o`.
+__device__ __forceinline__ uint32_t ld_outlier(const uint8_t* p, uint32_t o, uint32_t ob)
+{
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < ob; i++) m |= (uint32_t)p[o + i] << (8 * i);
+    return m;
+}
+
+// ------------------------------------------------------------------ block decode
+
+// Decodes the 1D block pair (rates rA, rB at payload offsets oA, oB of `pay`) into the
+// codes of this lane's elements (dA, dB).
+template <int MODE>
+__device__ __forceinline__ void decode_pair_1d(const uint8_t* pay, uint32_t rA, uint32_t rB, uint32_t oA, uint32_t oB,
+                                               int32_t& dA, int32_t& dB, int lane)
+{
+    uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
+    if constexpr (MODE == MODE_OUTLIER) {
+        nA = rA & 0x1f; nB = rB & 0x1f;
+        if (rA & 0x80) obA = ((rA & 0x60) >> 5) + 1;
+        if (rB & 0x80) obB = ((rB & 0x60) >> 5) + 1;
+    }
+    const bool hasA = payload_size<1, MODE>(rA) != 0, hasB = payload_size<1, MODE>(rB) != 0;
+    const uint32_t pA = oA + obA, pB = oB + obB;   // sign words
+    uint32_t magA = 0, magB = 0;
+    if (nA <= 16 && nB <= 16) {
+        const uint32_t p = lane & 15;
+        uint32_t w = 0;
+        if (lane < 16) { if (p < nA) w = lds32<MODE>(pay, pA + 4 + 4 * p); }
+        else           { if (p < nB) w = lds32<MODE>(pay, pB + 4 + 4 * p); }
+        if (nA | nB) {
+            const uint32_t x = warp_transpose32(from_stream_word(w), lane);
+            magA = x & 0xffffu;
+            magB = x >> 16;
+        }
+    } else {
+        const uint32_t wA = (uint32_t)lane < nA ? lds32<MODE>(pay, pA + 4 + 4 * lane) : 0u;
+        const uint32_t wB = (uint32_t)lane < nB ? lds32<MODE>(pay, pB + 4 + 4 * lane) : 0u;
+        magA = from_stream_word(wA);
+        magB = from_stream_word(wB);
+        warp_transpose32x2(magA, magB, lane);
+    }
+    if constexpr (MODE == MODE_OUTLIER) {
+        if (lane == 0) {
+            if (obA) magA = ld_outlier(pay, oA, obA);
+            if (obB) magB = ld_outlier(pay, oB, obB);
+        }
+    }
+    const uint32_t sA = hasA ? from_stream_word(lds32<MODE>(pay, pA)) : 0u;
+    const uint32_t sB = hasB ? from_stream_word(lds32<MODE>(pay, pB)) : 0u;
+    dA = hasA ? (((sA >> lane) & 1u) ? (int32_t)(0u - magA) : (int32_t)magA) : 0;
+    dB = hasB ? (((sB >> lane) & 1u) ? (int32_t)(0u - magB) : (int32_t)magB) : 0;
+}
+
+// Decodes one 2D/3D block (rate r at payload offset o) into the codes of this lane's
+// two elements (d0: element lane, d1: element lane + 32).
+template <int MODE>
+__device__ __forceinline__ void decode_block_nd(const uint8_t* pay, uint32_t r, uint32_t o, int32_t& d0, int32_t& d1,
+                                                int lane)
+{
+    if (payload_size<2, MODE>(r) == 0) { d0 = 0; d1 = 0; return; }
+    uint32_t n = r, ob = 0;
+    if constexpr (MODE == MODE_OUTLIER) {
+        n = r & 0x1f;
+        if (r & 0x80) ob = ((r & 0x60) >> 5) + 1;
+    }
+    const uint32_t p = o + ob;   // sign words
+    uint32_t mag0, mag1;
+    if (n <= 16) {
+        const uint32_t pl = lane & 15;
+        const uint32_t w = pl < n ? lds32<MODE>(pay, p + 8 + 8 * pl + (lane >> 4) * 4) : 0u;
+        const uint32_t x = warp_transpose32(from_stream_word(w), lane);
+        mag0 = x & 0xffffu;
+        mag1 = x >> 16;
+    } else {
+        mag0 = (uint32_t)lane < n ? from_stream_word(lds32<MODE>(pay, p + 8 + 8 * lane)) : 0u;
+        mag1 = (uint32_t)lane < n ? from_stream_word(lds32<MODE>(pay, p + 12 + 8 * lane)) : 0u;
+        warp_transpose32x2(mag0, mag1, lane);
+    }
+    if constexpr (MODE == MODE_OUTLIER) {
+        if (ob && lane == 0) mag0 = ld_outlier(pay, o, ob);
+    }
+    const uint32_t s0 = from_stream_word(lds32<MODE>(pay, p)), s1 = from_stream_word(lds32<MODE>(pay, p + 4));
+    d0 = ((s0 >> lane) & 1u) ? (int32_t)(0u - mag0) : (int32_t)mag0;
+    d1 = ((s1 >> lane) & 1u) ? (int32_t)(0u - mag1) : (int32_t)mag1;
+}
+
+// ------------------------------------------------------------------ TMA stores
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+                 : "memory");
+}
+// `bytes` (a multiple of 16) from shared `src` to global `dst` (16-byte aligned).
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// ------------------------------------------------------------------ the kernel
+
+template <typename T, int DIM, int MODE>
+__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
+decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const uint8_t* __restrict__ cmp,
+                      Geom g, T eb, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+{
+    using C = DecCfg<T, DIM>;
+    extern __shared__ unsigned char dsm[];
+    unsigned char* base = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
+    uint8_t* slots = base + C::OFF_SLOT;
+    T* obuf = reinterpret_cast<T*>(base + C::OFF_OUT);
+    __shared__ __align__(8) DecShared<T, DIM> sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* err = &hdr->err;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < C::FRONT; i++) {
+            mbar_init(&sh.full[i], 1);
+            mbar_init(&sh.freed[i], C::WARPS);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    if (warp >= C::WARPS) {
+        // ---------------------------------------------------------------- front warps
+        const int f = warp - C::WARPS;
+        uint8_t* slot = slots + f * C::SLOT;
+        for (int m = 0;; m++) {
+            if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) break;
+            int64_t t = 0;
+            if (lane == 0) t = (int64_t)atomicAdd(&hdr->ticket, 1u);
+            t = __shfl_sync(FULL, t, 0);
+            if ((uint64_t)t >= g.ntiles) {
+                if (lane == 0) {
+                    sh.tile[f] = t;
+                    mbar_arrive(&sh.full[f]);
+                }
+                break;
+            }
+            // rate bytes -> block sizes -> codec warp offsets and the tile aggregate
+            const uint64_t b0 = (uint64_t)t * C::TB;
+            constexpr int PER = C::TB / 32;   // rate bytes per lane (4 in 1D, 2 in 2D/3D)
+            uint32_t sz[PER], rsum = 0;
+#pragma unroll
+            for (int i = 0; i < PER; i++) {
+                const uint64_t b = b0 + (uint64_t)lane * PER + i;   // lane holds consecutive blocks
+                const uint32_t r = b < g.nblocks ? __ldg(cmp + b) : 0u;
+                sh.rates[f][lane * PER + i] = (uint8_t)r;
+                sz[i] = payload_size<DIM, MODE>(r);
+                rsum += sz[i];
+            }
+            uint32_t incl = rsum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const unsigned long long agg = __shfl_sync(FULL, incl, 31);
+            // codec warp w starts at block w * BPW = lane (w * BPW / PER)'s first block
+            constexpr int LPW = C::BPW / PER;   // lanes per codec warp
+            if (lane % LPW == 0) sh.woff[f][lane / LPW] = incl - rsum;
+            __syncwarp();   // rates and offsets are written before lane 0 publishes the slot
+            if (lane == 0) st_release(status + t, (t == 0 ? ST_INC : ST_AGG) | agg);
+            const uint64_t excl = t > 0 ? warp_lookback(status, t, err) : 0;
+            if (lane == 0) {
+                if (t > 0) st_release(status + t, ST_INC | ((excl + agg) & ST_VAL));
+                if ((uint64_t)t == g.ntiles - 1) hdr->total = g.rate_bytes + excl + agg;
+                const uint64_t p0 = g.rate_bytes + excl, p1 = p0 + agg;
+                const uint64_t a0 = p0 & ~15ull, a1 = (p1 + 15) & ~15ull;
+                // rate bytes no valid stream holds (rate > 32 outside outlier mode) could
+                // claim more than a slot: such a tile is not loaded and decodes to zeros
+                const bool fits = agg <= (unsigned long long)C::TB * C::MAXBLK;
+                if (!fits) atomicOr(err, ERR_CAPACITY);
+                const uint32_t bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
+                sh.tile[f] = t;
+                sh.poff[f] = fits ? (uint32_t)(p0 - a0) : kBadSlot;
+                mbar_arrive_tx(&sh.full[f], bytes);
+                if (bytes) bulk_load(slot, cmp + a0, bytes, &sh.full[f]);
+            }
+            __syncwarp();
+        }
+    } else {
+        // ---------------------------------------------------------------- codec warps
+        T* ob = obuf + warp * (C::BPW * C::BLK);
+        uint32_t parity = 0;      // bit f: phase parity of slot f's next fill
+        uint32_t ended = 0;       // bit f: front warp f has no more tiles
+        bool stored = false;      // this warp has bulk stores in flight
+        for (int k = 0; ended != (1u << C::FRONT) - 1u; k++) {
+            const int f = k % C::FRONT;
+            if ((ended >> f) & 1u) continue;
+            const uint32_t ph = (parity >> f) & 1u;
+            parity ^= 1u << f;
+            if (!mbar_wait(&sh.full[f], ph, err)) break;
+            const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tile[f]);
+            if ((uint64_t)t >= g.ntiles) { ended |= 1u << f; continue; }
+            const uint8_t* pay = slots + f * C::SLOT;
+            const bool bad = sh.poff[f] == kBadSlot;
+            // this warp's blocks: rate bytes, payload offsets (lane j: block j)
+            const uint32_t myr = lane < C::BPW && !bad ? sh.rates[f][warp * C::BPW + lane] : 0u;
+            const uint32_t mysz = lane < C::BPW ? payload_size<DIM, MODE>(myr) : 0u;
+            uint32_t incl = mysz;
+#pragma unroll
+            for (int o = 1; o < C::BPW; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][warp] + incl - mysz;
+            // the output buffer is free once the previous stores have read it
+            if (stored && lane == 0) bulk_wait_read();
+            __syncwarp();
+            const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
+            if constexpr (DIM == 1) {
+#pragma unroll 1
+                for (int j = 0; j < C::BPW; j += 2) {
+                    const uint32_t rA = __shfl_sync(FULL, myr, j), rB = __shfl_sync(FULL, myr, j + 1);
+                    const uint32_t oA = __shfl_sync(FULL, myo, j), oB = __shfl_sync(FULL, myo, j + 1);
+                    int32_t dA, dB;
+                    decode_pair_1d<MODE>(pay, rA, rB, oA, oB, dA, dB, lane);
+                    if constexpr (MODE != MODE_FIXED) {
+                        int32_t z = 0;
+                        lorenzo_inverse<1>(dA, z, lane);
+                        lorenzo_inverse<1>(dB, z, lane);
+                    }
+                    // blocks without payload decode to 0.0
+                    ob[j * 32 + lane] = payload_size<1, MODE>(rA) ? dequant(dA, eb) : T(0);
+                    ob[(j + 1) * 32 + lane] = payload_size<1, MODE>(rB) ? dequant(dB, eb) : T(0);
+                }
+            } else {
+#pragma unroll 1
+                for (int j = 0; j < C::BPW; j++) {
+                    const uint32_t r = __shfl_sync(FULL, myr, j), o = __shfl_sync(FULL, myo, j);
+                    int32_t d0, d1;
+                    decode_block_nd<MODE>(pay, r, o, d0, d1, lane);
+                    if constexpr (MODE != MODE_FIXED) lorenzo_inverse<DIM>(d0, d1, lane);
+                    const bool z = payload_size<DIM, MODE>(r) == 0;
+                    ob[j * 64 + lane] = z ? T(0) : dequant(d0, eb);
+                    ob[j * 64 + 32 + lane] = z ? T(0) : dequant(d1, eb);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sh.freed[f]);   // done with the payload slot
+            fence_proxy_async_smem();                  // decoded values -> async proxy
+            __syncwarp();
+            if constexpr (DIM == 1) {
+                // the warp's 512 contiguous elements, clipped to the array
+                const uint64_t e0 = b0 * 32;
+                const uint64_t cnt = e0 < g.nbEle ? min((uint64_t)(C::BPW * 32), g.nbEle - e0) : 0;
+                const uint32_t bytes = (uint32_t)cnt * (uint32_t)sizeof(T);
+                const uint32_t main = bytes & ~15u;
+                const uint32_t tail = (bytes - main) / (uint32_t)sizeof(T);
+                if ((uint32_t)lane < tail) out[e0 + main / sizeof(T) + lane] = ob[main / sizeof(T) + lane];
+                if (lane == 0 && main) {
+                    bulk_store(out + e0, ob, main);
+                    bulk_commit();
+                    stored = true;
+                }
+            } else {
+                if (lane == 0 && b0 < g.nblocks) {
+                    const uint32_t nb = (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0);
+                    for (uint32_t j = 0; j < nb; j++) {
+                        const BlockPos p = block_pos(b0 + j, g);
+                        if constexpr (DIM == 2)
+                            tma_store_3d(&tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, ob + j * 64);
+                        else
+                            tma_store_3d(&tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob + j * 64);
+                    }
+                    bulk_commit();
+                    stored = true;
+                }
+            }
+            __syncwarp();
+        }
+        if (lane == 0 && stored) bulk_wait_all();
+        __syncwarp();
+    }
+    finish_cta(hdr, status, g.ntiles);
+}
+
+}  // namespace cuszp

@@ -154,7 +154,8 @@ MISALIGNED_SHAPES = [(1, (0, 0, 0), 100_003), (2, (516, 301, 2), None), (3, (68,
 @pytest.mark.parametrize("dim,dims,n", MISALIGNED_SHAPES, ids=lambda v: str(v))
 def test_input_off_16_byte_boundary_matches_oracle(dtype, mode, dim, dims, n):
     """Inputs that do not start on a 16-byte boundary (an element-offset view) take the
-    per-element cp.async compress kernel instead of the TMA one: same bytes."""
+    per-element cp.async compress kernel instead of the TMA one, and outputs off the
+    boundary the per-warp decompress kernel: same bytes, same reconstruction."""
     from cuszp_b200 import codec
     rng = np.random.default_rng(dim * 10 + mode)
     if n is None:
@@ -175,6 +176,10 @@ def test_input_off_16_byte_boundary_matches_oracle(dtype, mode, dim, dims, n):
     S = int(size.item())
     assert S == want.size
     assert np.array_equal(out[:S].cpu().numpy(), want)
+    rec = torch.full((n + 1,), float("nan"), dtype=TT[dtype], device="cuda")
+    codec.decompress_into(out, rec[1:], eb, mode, dim, lay.dims)
+    exp = O.decompress(want, n, dtype, eb, mode, dim, dims)
+    assert np.array_equal(rec[1:].cpu().numpy().view(np.uint8), exp.view(np.uint8))
 
 
 # --------------------------------------------------------------------------- edge cases
