@@ -229,23 +229,26 @@ template <int DIM, int MODE>
 __device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lane)
 {
     constexpr int W = DIM == 1 ? 4 : 8;
-    uint32_t m, m2 = 0;
-    if constexpr (DIM == 1) {
-        m = (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
-        if constexpr (MODE == MODE_OUTLIER) m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
-    } else {
-        m = __reduce_max_sync(FULL, max(a0, a1));
-        if constexpr (MODE == MODE_OUTLIER) m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
-    }
-    const int fr1 = bitlen(m);
     if constexpr (MODE == MODE_OUTLIER) {
+        // maxima without element 0 (m2) and with it (m, from m2 and element 0 itself)
+        const uint32_t o = __shfl_sync(FULL, a0, 0);
+        uint32_t m, m2;
+        if constexpr (DIM == 1) {
+            m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
+            m = (uint32_t)max((int)m2, (int)o);
+        } else {
+            m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
+            m = max(m2, o);
+        }
+        const int fr1 = bitlen(m);
         const int fr2 = bitlen(m2);
-        const int ob = (bitlen(__shfl_sync(FULL, a0, 0)) + 7) / 8;
+        const int ob = (bitlen(o) + 7) / 8;
         const int cost1 = fr1 ? W + fr1 * W : 0;
         const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
         return cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
     } else {
-        return (uint32_t)fr1;
+        if constexpr (DIM == 1) return (uint32_t)bitlen((uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0));
+        else return (uint32_t)bitlen(__reduce_max_sync(FULL, max(a0, a1)));
     }
 }
 

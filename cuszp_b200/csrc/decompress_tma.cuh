@@ -69,12 +69,12 @@ __device__ __forceinline__ uint32_t lds32(const uint8_t* p, uint32_t o)
         return *reinterpret_cast<const uint32_t*>(p + o);
     }
 }
-// Element 0's magnitude stored in `ob` little-endian bytes at offset `o`.
+// Element 0's magnitude stored in `ob` (1..4) little-endian bytes at offset `o`: one
+// unaligned word read, masked (the bytes after it belong to the same payload).
 __device__ __forceinline__ uint32_t ld_outlier(const uint8_t* p, uint32_t o, uint32_t ob)
 {
-    uint32_t m = 0;
-    for (uint32_t i = 0; i < ob; i++) m |= (uint32_t)p[o + i] << (8 * i);
-    return m;
+    const uint32_t w = lds32<MODE_OUTLIER>(p, o);
+    return ob >= 4 ? w : w & ((1u << (8 * ob)) - 1u);
 }
 
 // ------------------------------------------------------------------ block decode
@@ -154,6 +154,45 @@ __device__ __forceinline__ void decode_block_nd(const uint8_t* pay, uint32_t r, 
     const uint32_t s0 = from_stream_word(lds32<MODE>(pay, p)), s1 = from_stream_word(lds32<MODE>(pay, p + 4));
     d0 = ((s0 >> lane) & 1u) ? (int32_t)(0u - mag0) : (int32_t)mag0;
     d1 = ((s1 >> lane) & 1u) ? (int32_t)(0u - mag1) : (int32_t)mag1;
+}
+
+// Two 2D/3D blocks at once: when both have payloads of rate <= 16 their transposes run
+// interleaved; otherwise one after the other.
+template <int MODE>
+__device__ __forceinline__ void decode_pair_nd(const uint8_t* pay, uint32_t ra, uint32_t rb, uint32_t oa, uint32_t ob_,
+                                               int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane)
+{
+    uint32_t na = ra, nb = rb, oba = 0, obb = 0;
+    if constexpr (MODE == MODE_OUTLIER) {
+        na = ra & 0x1f; nb = rb & 0x1f;
+        if (ra & 0x80) oba = ((ra & 0x60) >> 5) + 1;
+        if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
+    }
+    if (na > 16 || nb > 16 || payload_size<2, MODE>(ra) == 0 || payload_size<2, MODE>(rb) == 0) {
+        decode_block_nd<MODE>(pay, ra, oa, d0a, d1a, lane);
+        decode_block_nd<MODE>(pay, rb, ob_, d0b, d1b, lane);
+        return;
+    }
+    const uint32_t pa = oa + oba, pb = ob_ + obb;   // sign words
+    const uint32_t pl = lane & 15, h4 = (uint32_t)(lane >> 4) * 4;
+    uint32_t xa = pl < na ? lds32<MODE>(pay, pa + 8 + 8 * pl + h4) : 0u;
+    uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : 0u;
+    xa = from_stream_word(xa);
+    xb = from_stream_word(xb);
+    warp_transpose32x2(xa, xb, lane);
+    uint32_t m0a = xa & 0xffffu, m1a = xa >> 16, m0b = xb & 0xffffu, m1b = xb >> 16;
+    if constexpr (MODE == MODE_OUTLIER) {
+        if (lane == 0) {
+            if (oba) m0a = ld_outlier(pay, oa, oba);
+            if (obb) m0b = ld_outlier(pay, ob_, obb);
+        }
+    }
+    const uint32_t s0a = from_stream_word(lds32<MODE>(pay, pa)), s1a = from_stream_word(lds32<MODE>(pay, pa + 4));
+    const uint32_t s0b = from_stream_word(lds32<MODE>(pay, pb)), s1b = from_stream_word(lds32<MODE>(pay, pb + 4));
+    d0a = ((s0a >> lane) & 1u) ? (int32_t)(0u - m0a) : (int32_t)m0a;
+    d1a = ((s1a >> lane) & 1u) ? (int32_t)(0u - m1a) : (int32_t)m1a;
+    d0b = ((s0b >> lane) & 1u) ? (int32_t)(0u - m0b) : (int32_t)m0b;
+    d1b = ((s1b >> lane) & 1u) ? (int32_t)(0u - m1b) : (int32_t)m1b;
 }
 
 // ------------------------------------------------------------------ TMA stores
@@ -286,7 +325,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
             }
             const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][warp] + incl - mysz;
             // the output buffer is free once the previous stores have read it
-            if (stored && lane == 0) bulk_wait_read();
+            if (stored) bulk_wait_read();
             __syncwarp();
             const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
             if constexpr (DIM == 1) {
@@ -307,14 +346,20 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                 }
             } else {
 #pragma unroll 1
-                for (int j = 0; j < C::BPW; j++) {
-                    const uint32_t r = __shfl_sync(FULL, myr, j), o = __shfl_sync(FULL, myo, j);
-                    int32_t d0, d1;
-                    decode_block_nd<MODE>(pay, r, o, d0, d1, lane);
-                    if constexpr (MODE != MODE_FIXED) lorenzo_inverse<DIM>(d0, d1, lane);
-                    const bool z = payload_size<DIM, MODE>(r) == 0;
-                    ob[j * 64 + lane] = z ? T(0) : dequant(d0, eb);
-                    ob[j * 64 + 32 + lane] = z ? T(0) : dequant(d1, eb);
+                for (int j = 0; j < C::BPW; j += 2) {
+                    const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
+                    const uint32_t rb = __shfl_sync(FULL, myr, j + 1), obo = __shfl_sync(FULL, myo, j + 1);
+                    int32_t d0a, d1a, d0b, d1b;
+                    decode_pair_nd<MODE>(pay, ra, rb, oa, obo, d0a, d1a, d0b, d1b, lane);
+                    if constexpr (MODE != MODE_FIXED) {
+                        lorenzo_inverse<DIM>(d0a, d1a, lane);
+                        lorenzo_inverse<DIM>(d0b, d1b, lane);
+                    }
+                    const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb) == 0;
+                    ob[j * 64 + lane] = za ? T(0) : dequant(d0a, eb);
+                    ob[j * 64 + 32 + lane] = za ? T(0) : dequant(d1a, eb);
+                    ob[j * 64 + 64 + lane] = zb ? T(0) : dequant(d0b, eb);
+                    ob[j * 64 + 96 + lane] = zb ? T(0) : dequant(d1b, eb);
                 }
             }
             __syncwarp();
@@ -335,22 +380,21 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                     stored = true;
                 }
             } else {
-                if (lane == 0 && b0 < g.nblocks) {
-                    const uint32_t nb = (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0);
-                    for (uint32_t j = 0; j < nb; j++) {
-                        const BlockPos p = block_pos(b0 + j, g);
-                        if constexpr (DIM == 2)
-                            tma_store_3d(&tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, ob + j * 64);
-                        else
-                            tma_store_3d(&tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob + j * 64);
-                    }
+                // lane j stores block j (bulk groups are per thread: each storing lane
+                // commits and later waits for its own)
+                if ((uint64_t)lane < C::BPW && b0 + lane < g.nblocks) {
+                    const BlockPos p = block_pos(b0 + lane, g);
+                    if constexpr (DIM == 2)
+                        tma_store_3d(&tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, ob + lane * 64);
+                    else
+                        tma_store_3d(&tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob + lane * 64);
                     bulk_commit();
                     stored = true;
                 }
             }
             __syncwarp();
         }
-        if (lane == 0 && stored) bulk_wait_all();
+        if (stored) bulk_wait_all();
         __syncwarp();
     }
     finish_cta(hdr, status, g.ntiles);
