@@ -101,6 +101,54 @@ __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p);
 __device__ __forceinline__ void st_stream(float* p, float v) { __stcs(p, v); }
 __device__ __forceinline__ void st_stream(double* p, double v) { __stcs(p, v); }
 
+// ------------------------------------------------------------------ shared-memory access
+
+// Shared memory addressed through 32-bit shared-window addresses: address arithmetic
+// stays 32-bit and the accesses compile to LDS/STS whatever the compiler can prove
+// about a pointer's origin.  Volatile with a memory clobber: they are never moved
+// across mbarrier waits or warp barriers.
+using saddr_t = uint32_t;
+__device__ __forceinline__ saddr_t saddr(const void* p) { return (saddr_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void sts_u8(saddr_t a, uint32_t v)
+{
+    asm volatile("st.shared.u8 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void sts_u16(saddr_t a, uint32_t v)
+{
+    asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((unsigned short)v) : "memory");
+}
+__device__ __forceinline__ void sts_u32(saddr_t a, uint32_t v)
+{
+    asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t lds_u8(saddr_t a)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t lds_u32(saddr_t a)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ void sts_val(saddr_t a, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
+__device__ __forceinline__ void sts_val(saddr_t a, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory"); }
+template <typename T> __device__ __forceinline__ T lds_val(saddr_t a);
+template <> __device__ __forceinline__ float lds_val<float>(saddr_t a)
+{
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
+    return v;
+}
+template <> __device__ __forceinline__ double lds_val<double>(saddr_t a)
+{
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a) : "memory");
+    return v;
+}
+
 // ------------------------------------------------------------------ warp bit transpose
 
 // 32x32 bit-matrix transpose across a warp: on entry the lane whose row index is

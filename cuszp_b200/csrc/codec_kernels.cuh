@@ -32,13 +32,22 @@ template <int DIM, int WARPS_ = kWarps, int BPW_ = (DIM == 1 ? 16 : 8)> struct T
 
 // --------------------------------------------------------------- byte stores / loads
 
+// put32 into shared memory.  Outlier-mode words sit at any byte offset; the offset's
+// residue mod 4 is the same for every word of a block, so the branch is warp-uniform.
 template <int MODE>
-__device__ __forceinline__ void put32(uint8_t* p, uint32_t v)
+__device__ __forceinline__ void put32s(saddr_t a, uint32_t v)
 {
-    if constexpr (MODE == MODE_OUTLIER) {   // outlier payloads sit at any byte offset
-        p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
+    if constexpr (MODE == MODE_OUTLIER) {
+        if ((a & 3u) == 0) {
+            sts_u32(a, v);
+        } else if ((a & 1u) == 0) {
+            sts_u16(a, v);
+            sts_u16(a + 2, v >> 16);
+        } else {
+            sts_u8(a, v); sts_u8(a + 1, v >> 8); sts_u8(a + 2, v >> 16); sts_u8(a + 3, v >> 24);
+        }
     } else {
-        *reinterpret_cast<uint32_t*>(p) = v;
+        sts_u32(a, v);
     }
 }
 // Outlier-mode payload words sit at any byte offset: read the (at most two) aligned
@@ -260,8 +269,8 @@ __device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lan
 
 // Payload of two 1D blocks A and B (rates rA, rB; codes cA, cB of this lane) at pA / pB.
 template <int MODE>
-__device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t cA, int32_t cB, uint8_t* pA,
-                                             uint8_t* pB, int lane)
+__device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t cA, int32_t cB, saddr_t pA,
+                                             saddr_t pB, int lane)
 {
     uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -274,8 +283,8 @@ __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t c
         // element 0's magnitude, little-endian, one byte per lane (lanes 0-3: A, 4-7: B)
         const uint32_t oA = __shfl_sync(FULL, aA, 0), oB = __shfl_sync(FULL, aB, 0);
         const uint32_t i = lane & 3;
-        if (lane < 4 && i < obA) pA[i] = (uint8_t)(oA >> (8 * i));
-        if (lane >= 4 && lane < 8 && i < obB) pB[i] = (uint8_t)(oB >> (8 * i));
+        if (lane < 4 && i < obA) sts_u8(pA + i, oA >> (8 * i));
+        if (lane >= 4 && lane < 8 && i < obB) sts_u8(pB + i, oB >> (8 * i));
         if (lane == 0) {
             if (obA) aA = 0;
             if (obB) aB = 0;
@@ -292,28 +301,28 @@ __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t c
         const uint32_t p = (lane ^ 7) & 15;
         const bool b = lane >= 16;
         const uint32_t n = b ? nB : nA;
-        uint8_t* q = b ? pB : pA;
+        const saddr_t q = b ? pB : pA;
         if (p == 15) {
-            if (b ? hasB : hasA) put32<MODE>(q, y);
+            if (b ? hasB : hasA) put32s<MODE>(q, y);
         } else if (p < n) {
-            put32<MODE>(q + 4 + 4 * p, y);
+            put32s<MODE>(q + 4 + 4 * p, y);
         }
     } else {
         const uint32_t sA = to_stream_word(__ballot_sync(FULL, cA < 0));
         const uint32_t sB = to_stream_word(__ballot_sync(FULL, cB < 0));
-        if (lane == 0 && hasA) put32<MODE>(pA, sA);
-        if (lane == 16 && hasB) put32<MODE>(pB, sB);
-        const uint32_t yA = warp_transpose32(aA, lane ^ 7);
-        const uint32_t yB = warp_transpose32(aB, lane ^ 7);
+        if (lane == 0 && hasA) put32s<MODE>(pA, sA);
+        if (lane == 16 && hasB) put32s<MODE>(pB, sB);
+        uint32_t yA = aA, yB = aB;
+        warp_transpose32x2(yA, yB, lane ^ 7);
         const int p = lane ^ 7;
-        if ((uint32_t)p < nA) put32<MODE>(pA + 4 + 4 * p, yA);
-        if ((uint32_t)p < nB) put32<MODE>(pB + 4 + 4 * p, yB);
+        if ((uint32_t)p < nA) put32s<MODE>(pA + 4 + 4 * p, yA);
+        if ((uint32_t)p < nB) put32s<MODE>(pB + 4 + 4 * p, yB);
     }
 }
 
 // Payload of one 2D/3D block (rate r != 0; codes c0, c1 of this lane's two elements) at p.
 template <int MODE>
-__device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1, uint8_t* p, int lane)
+__device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1, saddr_t p, int lane)
 {
     uint32_t n = r, ob = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -325,7 +334,7 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
     if constexpr (MODE == MODE_OUTLIER) {
         // element 0's magnitude, little-endian, one byte per lane
         const uint32_t o = __shfl_sync(FULL, a0, 0);
-        if ((uint32_t)lane < ob) p[lane] = (uint8_t)(o >> (8 * lane));
+        if ((uint32_t)lane < ob) sts_u8(p + lane, o >> (8 * lane));
         if (lane == 0 && ob) a0 = 0;
         p += ob;
     }
@@ -336,18 +345,18 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
         const uint32_t y = warp_transpose32(x, lane ^ 7);
         const uint32_t pl = (lane ^ 7) & 15;
         const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
-        if (pl == 15) put32<MODE>(p + h4, y);
-        else if (pl < n) put32<MODE>(p + 8 + 8 * pl + h4, y);
+        if (pl == 15) put32s<MODE>(p + h4, y);
+        else if (pl < n) put32s<MODE>(p + 8 + 8 * pl + h4, y);
     } else {
         const uint32_t s0 = to_stream_word(__ballot_sync(FULL, c0 < 0));
         const uint32_t s1 = to_stream_word(__ballot_sync(FULL, c1 < 0));
-        if (lane < 2) put32<MODE>(p + 4 * lane, lane ? s1 : s0);
-        const uint32_t ylo = warp_transpose32(a0, lane ^ 7);
-        const uint32_t yhi = warp_transpose32(a1, lane ^ 7);
+        if (lane < 2) put32s<MODE>(p + 4 * lane, lane ? s1 : s0);
+        uint32_t ylo = a0, yhi = a1;
+        warp_transpose32x2(ylo, yhi, lane ^ 7);
         const int pl = lane ^ 7;
         if ((uint32_t)pl < n) {
-            put32<MODE>(p + 8 + 8 * pl, ylo);
-            put32<MODE>(p + 12 + 8 * pl, yhi);
+            put32s<MODE>(p + 8 + 8 * pl, ylo);
+            put32s<MODE>(p + 12 + 8 * pl, yhi);
         }
     }
 }
@@ -356,7 +365,7 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
 // blocks' transposes run interleaved when both rates are <= 15.
 template <int MODE>
 __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c0a, int32_t c1a, int32_t c0b,
-                                             int32_t c1b, uint8_t* pa, uint8_t* pb, int lane)
+                                             int32_t c1b, saddr_t pa, saddr_t pb, int lane)
 {
     uint32_t na = ra, nb = rb, oba = 0, obb = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -375,8 +384,8 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
         // element 0's magnitude, little-endian, one byte per lane (lanes 0-3: a, 4-7: b)
         const uint32_t oa = __shfl_sync(FULL, a0a, 0), ob = __shfl_sync(FULL, a0b, 0);
         const uint32_t i = lane & 3;
-        if (lane < 4 && i < oba) pa[i] = (uint8_t)(oa >> (8 * i));
-        if (lane >= 4 && lane < 8 && i < obb) pb[i] = (uint8_t)(ob >> (8 * i));
+        if (lane < 4 && i < oba) sts_u8(pa + i, oa >> (8 * i));
+        if (lane >= 4 && lane < 8 && i < obb) sts_u8(pb + i, ob >> (8 * i));
         if (lane == 0) {
             if (oba) a0a = 0;
             if (obb) a0b = 0;
@@ -392,8 +401,8 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
     const uint32_t pl = (lane ^ 7) & 15;
     const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
     const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
-    if (ra && (pl == 15 || pl < na)) put32<MODE>(pa + o, xa);
-    if (rb && (pl == 15 || pl < nb)) put32<MODE>(pb + o, xb);
+    if (ra && (pl == 15 || pl < na)) put32s<MODE>(pa + o, xa);
+    if (rb && (pl == 15 || pl < nb)) put32s<MODE>(pb + o, xb);
 }
 
 // Sign maps and bit-planes of the warp's blocks at their final offsets.
@@ -407,15 +416,15 @@ __device__ __forceinline__ void compress_pack(const CompressWork<T, DIM, Tl>& K,
         for (int j = 0; j < BPW; j += 2) {
             const uint32_t rA = __shfl_sync(FULL, K.myrb, j), rB = __shfl_sync(FULL, K.myrb, j + 1);
             if ((rA | rB) == 0) continue;
-            pack_pair_1d<MODE>(rA, rB, K.c0[j], K.c0[j + 1], pbase + __shfl_sync(FULL, K.myoff, j),
-                               pbase + __shfl_sync(FULL, K.myoff, j + 1), lane);
+            pack_pair_1d<MODE>(rA, rB, K.c0[j], K.c0[j + 1], saddr(pbase) + __shfl_sync(FULL, K.myoff, j),
+                               saddr(pbase) + __shfl_sync(FULL, K.myoff, j + 1), lane);
         }
     } else {
 #pragma unroll
         for (int j = 0; j < BPW; j++) {
             const uint32_t r = __shfl_sync(FULL, K.myrb, j);
             if (r == 0) continue;
-            pack_block_nd<MODE>(r, K.c0[j], K.c1[DIM == 1 ? 0 : j], pbase + __shfl_sync(FULL, K.myoff, j), lane);
+            pack_block_nd<MODE>(r, K.c0[j], K.c1[DIM == 1 ? 0 : j], saddr(pbase) + __shfl_sync(FULL, K.myoff, j), lane);
         }
     }
 }

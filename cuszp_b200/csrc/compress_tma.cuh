@@ -157,21 +157,20 @@ struct TmaShared {
 // 1D: codes of the warp's 16 blocks of tile `t` (elements in `tin`) into `code`, their
 // rate bytes to the stream and to `rates`; returns the warp's payload bytes.
 template <typename T, int MODE>
-__device__ __forceinline__ uint32_t rate_pass_1d(const T* __restrict__ tin, int32_t* __restrict__ code,
-                                                 uint8_t* __restrict__ rates, int warp, int64_t t, const Geom& g,
-                                                 T recip, uint8_t* __restrict__ cmp, int lane)
+__device__ __forceinline__ uint32_t rate_pass_1d(saddr_t tin, saddr_t code, saddr_t rates, int warp, int64_t t,
+                                                 const Geom& g, T recip, uint8_t* __restrict__ cmp, int lane)
 {
     using C = TmaCfg<T, 1>;
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
     uint32_t off = 0, rb = 0;
     if (b0 * 32 < g.nbEle) {
-        const T* wb = tin + warp * C::BPW * 32;
-        int32_t* wc = code + warp * C::BPW * 32;
+        const saddr_t wb = tin + (warp * C::BPW * 32 + lane) * (uint32_t)sizeof(T);
+        const saddr_t wc = code + (warp * C::BPW * 32 + lane) * 4u;
         const bool ragged = (b0 + C::BPW) * 32 > g.nbEle;
 #pragma unroll 2
         for (int j = 0; j < C::BPW; j += 2) {
-            const int32_t qA = quantize(wb[j * 32 + lane], recip);
-            const int32_t qB = quantize(wb[(j + 1) * 32 + lane], recip);
+            const int32_t qA = quantize(lds_val<T>(wb + j * 32 * sizeof(T)), recip);
+            const int32_t qB = quantize(lds_val<T>(wb + (j + 1) * 32 * sizeof(T)), recip);
             int32_t cA = qA, cB = qB;
             if constexpr (MODE != MODE_FIXED) {
                 const int32_t uA = __shfl_up_sync(FULL, qA, 1), uB = __shfl_up_sync(FULL, qB, 1);
@@ -183,8 +182,8 @@ __device__ __forceinline__ uint32_t rate_pass_1d(const T* __restrict__ tin, int3
                 cA = i < g.nbEle ? cA : 0;
                 cB = i + 32 < g.nbEle ? cB : 0;
             }
-            wc[j * 32 + lane] = cA;
-            wc[(j + 1) * 32 + lane] = cB;
+            sts_u32(wc + j * 128, (uint32_t)cA);
+            sts_u32(wc + (j + 1) * 128, (uint32_t)cB);
             const uint32_t rA = block_rate<1, MODE>(uabs(cA), 0u, lane);
             const uint32_t rB = block_rate<1, MODE>(uabs(cB), 0u, lane);
             if (lane == j) rb = rA;
@@ -193,7 +192,7 @@ __device__ __forceinline__ uint32_t rate_pass_1d(const T* __restrict__ tin, int3
         }
     }
     if (lane < C::BPW) {
-        rates[warp * C::BPW + lane] = (uint8_t)rb;
+        sts_u8(rates + warp * C::BPW + lane, rb);
         if (b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)rb;
     }
     return off;
@@ -202,9 +201,8 @@ __device__ __forceinline__ uint32_t rate_pass_1d(const T* __restrict__ tin, int3
 // 2D/3D: same for the warp's 8 blocks (each block's 64 elements contiguous in `tin`),
 // two blocks per step so that their dependency chains overlap.
 template <typename T, int DIM, int MODE>
-__device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int32_t* __restrict__ code,
-                                                 uint8_t* __restrict__ rates, int warp, int64_t t, const Geom& g,
-                                                 T recip, uint8_t* __restrict__ cmp, int lane)
+__device__ __forceinline__ uint32_t rate_pass_nd(saddr_t tin, saddr_t code, saddr_t rates, int warp, int64_t t,
+                                                 const Geom& g, T recip, uint8_t* __restrict__ cmp, int lane)
 {
     using C = TmaCfg<T, DIM>;
     constexpr uint32_t B = DIM == 2 ? 8 : 4;
@@ -212,8 +210,8 @@ __device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int3
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
     uint32_t off = 0, rbyte = 0;
     if (b0 < g.nblocks) {
-        const T* wb = tin + warp * C::BPW * 64;
-        int32_t* wc = code + warp * C::BPW * 64;
+        const saddr_t wb = tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);   // this lane's element
+        const saddr_t wc = code + (warp * C::BPW * 64 + lane) * 4u;
         const BlockPos bp = block_pos(b0, g);
         uint32_t bx = bp.x, by = bp.y, bz = bp.z;
         // this lane's element coordinates inside a block (halves 0 and 1)
@@ -232,9 +230,9 @@ __device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int3
             }
         };
         // codes of one block (elements outside the array: code 0)
-        auto codes = [&](const T* blk, uint32_t x, uint32_t y, uint32_t z, int32_t& c0, int32_t& c1) {
-            const int32_t q0 = quantize(blk[lane], recip);
-            const int32_t q1 = quantize(blk[32 + lane], recip);
+        auto codes = [&](saddr_t blk, uint32_t x, uint32_t y, uint32_t z, int32_t& c0, int32_t& c1) {
+            const int32_t q0 = quantize(lds_val<T>(blk), recip);
+            const int32_t q1 = quantize(lds_val<T>(blk + 32 * sizeof(T)), recip);
             c0 = q0;
             c1 = q1;
             if constexpr (MODE != MODE_FIXED) {
@@ -257,14 +255,14 @@ __device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int3
             uint32_t xb2 = bx, yb2 = by, zb2 = bz;
             advance(xb2, yb2, zb2);
             int32_t c0a, c1a, c0b, c1b;
-            codes(wb + j * 64, bx, by, bz, c0a, c1a);
-            codes(wb + (j + 1) * 64, xb2, yb2, zb2, c0b, c1b);   // inside the warp's 8 blocks
+            codes(wb + j * 64 * sizeof(T), bx, by, bz, c0a, c1a);
+            codes(wb + (j + 1) * 64 * sizeof(T), xb2, yb2, zb2, c0b, c1b);   // inside the warp's 8 blocks
             if (j + 1 >= nblk) { c0b = 0; c1b = 0; }             // past the last block: rate 0
-            int32_t* ca = wc + j * 64;
-            ca[lane] = c0a;
-            ca[32 + lane] = c1a;
-            ca[64 + lane] = c0b;
-            ca[96 + lane] = c1b;
+            const saddr_t ca = wc + j * 256;
+            sts_u32(ca, (uint32_t)c0a);
+            sts_u32(ca + 128, (uint32_t)c1a);
+            sts_u32(ca + 256, (uint32_t)c0b);
+            sts_u32(ca + 384, (uint32_t)c1b);
             const uint32_t ra = block_rate<DIM, MODE>(uabs(c0a), uabs(c1a), lane);
             const uint32_t rb = block_rate<DIM, MODE>(uabs(c0b), uabs(c1b), lane);
             if (lane == (int)j) rbyte = ra;
@@ -275,7 +273,7 @@ __device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int3
         }
     }
     if (lane < C::BPW) {
-        rates[warp * C::BPW + lane] = (uint8_t)rbyte;
+        sts_u8(rates + warp * C::BPW + lane, rbyte);
         if (b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)rbyte;
     }
     return off;
@@ -286,11 +284,10 @@ __device__ __forceinline__ uint32_t rate_pass_nd(const T* __restrict__ tin, int3
 // Sign maps and bit-planes of the warp's blocks (codes in `code`, rate bytes in
 // `rates`) into `region`; returns the payload bytes written there.
 template <int DIM, int MODE, typename C>
-__device__ __forceinline__ uint32_t pack_pass(const int32_t* __restrict__ code, const uint8_t* __restrict__ rates,
-                                              int warp, uint8_t* __restrict__ region, int lane)
+__device__ __forceinline__ uint32_t pack_pass(saddr_t code, saddr_t rates, int warp, saddr_t region, int lane)
 {
-    const int32_t* wc = code + warp * C::BPW * C::BLK;
-    const uint32_t mine = lane < C::BPW ? rates[warp * C::BPW + lane] : 0u;
+    const saddr_t wc = code + (warp * C::BPW * C::BLK + lane) * 4u;   // this lane's code of block 0
+    const uint32_t mine = lane < C::BPW ? lds_u8(rates + warp * C::BPW + lane) : 0u;
     uint32_t off = 0;
 #pragma unroll 1
     for (int j = 0; j < C::BPW; j += 2) {
@@ -298,12 +295,12 @@ __device__ __forceinline__ uint32_t pack_pass(const int32_t* __restrict__ code, 
         const uint32_t sa = payload_size<DIM, MODE>(ra);
         if (ra | rb) {
             if constexpr (DIM == 1) {
-                pack_pair_1d<MODE>(ra, rb, wc[j * 32 + lane], wc[(j + 1) * 32 + lane], region + off, region + off + sa,
-                                   lane);
+                pack_pair_1d<MODE>(ra, rb, (int32_t)lds_u32(wc + j * 128), (int32_t)lds_u32(wc + (j + 1) * 128),
+                                   region + off, region + off + sa, lane);
             } else {
-                const int32_t* ca = wc + j * 64;
-                pack_pair_nd<MODE>(ra, rb, ca[lane], ca[32 + lane], ca[64 + lane], ca[96 + lane], region + off,
-                                   region + off + sa, lane);
+                const saddr_t ca = wc + j * 256;
+                pack_pair_nd<MODE>(ra, rb, (int32_t)lds_u32(ca), (int32_t)lds_u32(ca + 128), (int32_t)lds_u32(ca + 256),
+                                   (int32_t)lds_u32(ca + 384), region + off, region + off + sa, lane);
             }
         }
         off += sa + payload_size<DIM, MODE>(rb);
@@ -314,8 +311,7 @@ __device__ __forceinline__ uint32_t pack_pass(const int32_t* __restrict__ code, 
 // Warp-cooperative write of `n` staged bytes (`src` 16-byte aligned in shared memory)
 // to global `dst` (any alignment): 16-byte stores for the aligned units inside the
 // range, one byte store per lane for the ragged first and last units.
-__device__ __forceinline__ void warp_copy_out(const uint8_t* __restrict__ src, uint32_t n, uint8_t* __restrict__ dst,
-                                              int lane)
+__device__ __forceinline__ void warp_copy_out(saddr_t src, uint32_t n, uint8_t* __restrict__ dst, int lane)
 {
     if (n == 0) return;
     const uint32_t d = (uint32_t)((uintptr_t)dst & 15);
@@ -324,15 +320,16 @@ __device__ __forceinline__ void warp_copy_out(const uint8_t* __restrict__ src, u
     const uint32_t u1 = (d + n) >> 4;         // one past the last such unit
     for (uint32_t u = u0 + lane; u < u1; u += 32) {
         const uint32_t so = 16 * u - d;
-        const uint32_t* w = reinterpret_cast<const uint32_t*>(src + (so & ~3u));
+        const saddr_t w = src + (so & ~3u);
         const uint32_t sh = (so & 3u) * 8;
+        const uint32_t w0 = lds_u32(w), w1 = lds_u32(w + 4), w2 = lds_u32(w + 8), w3 = lds_u32(w + 12);
         uint4 v;
         if (sh == 0) {
-            v = make_uint4(w[0], w[1], w[2], w[3]);
+            v = make_uint4(w0, w1, w2, w3);
         } else {
-            const uint32_t w4 = w[4];
-            v = make_uint4(__funnelshift_r(w[0], w[1], sh), __funnelshift_r(w[1], w[2], sh),
-                           __funnelshift_r(w[2], w[3], sh), __funnelshift_r(w[3], w4, sh));
+            const uint32_t w4 = lds_u32(w + 16);
+            v = make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh), __funnelshift_r(w2, w3, sh),
+                           __funnelshift_r(w3, w4, sh));
         }
         __stcs(reinterpret_cast<uint4*>(first + 16 * u), v);
     }
@@ -343,7 +340,7 @@ __device__ __forceinline__ void warp_copy_out(const uint8_t* __restrict__ src, u
     const uint32_t unit = lane < 16 ? 0u : u1;
     if ((lane < 16 && head) || (lane >= 16 && tail)) {
         const uint32_t pos = 16 * unit + (uint32_t)(lane & 15);
-        if (pos >= d && pos < d + n) first[pos] = src[pos - d];
+        if (pos >= d && pos < d + n) first[pos] = (uint8_t)lds_u8(src + (pos - d));
     }
 }
 
@@ -475,11 +472,12 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
         __syncwarp();
     } else {
         // ---------------------------------------------------------------- codec warps
-        uint8_t* region = stg + warp * C::REGION;
+        const saddr_t region = saddr(stg + warp * C::REGION);
         auto pack_out = [&](int kk) -> bool {
             const int c = kk % C::NC;
             if (!mbar_wait(&sh.based[c], (uint32_t)(kk / C::NC) & 1u, err)) return false;
-            const uint32_t n = pack_pass<DIM, MODE, C>(codebuf + c * C::TILE_ELEMS, sh.rates[c], warp, region, lane);
+            const uint32_t n =
+                pack_pass<DIM, MODE, C>(saddr(codebuf + c * C::TILE_ELEMS), saddr(sh.rates[c]), warp, region, lane);
             __syncwarp();
             warp_copy_out(region, n, cmp + g.rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
             __syncwarp();
@@ -491,13 +489,13 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
             if (!mbar_wait(&sh.full[s], (uint32_t)(k / C::NIN) & 1u, err)) break;
             const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tick[s]);
             if ((uint64_t)t >= g.ntiles) break;
-            const T* tin = inbuf + s * C::TILE_ELEMS;
-            int32_t* code = codebuf + c * C::TILE_ELEMS;
+            const saddr_t tin = saddr(inbuf + s * C::TILE_ELEMS);
+            const saddr_t code = saddr(codebuf + c * C::TILE_ELEMS);
             uint32_t total;
             if constexpr (DIM == 1)
-                total = rate_pass_1d<T, MODE>(tin, code, sh.rates[c], warp, t, g, recip, cmp, lane);
+                total = rate_pass_1d<T, MODE>(tin, code, saddr(sh.rates[c]), warp, t, g, recip, cmp, lane);
             else
-                total = rate_pass_nd<T, DIM, MODE>(tin, code, sh.rates[c], warp, t, g, recip, cmp, lane);
+                total = rate_pass_nd<T, DIM, MODE>(tin, code, saddr(sh.rates[c]), warp, t, g, recip, cmp, lane);
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&sh.freed[s]);   // this warp is done with the input slot

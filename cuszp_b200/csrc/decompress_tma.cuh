@@ -59,19 +59,20 @@ struct DecShared {
 // Word at byte offset `o` of shared memory `p` (any alignment in outlier mode; the
 // payload of fixed/plain streams sits at 4-byte offsets).
 template <int MODE>
-__device__ __forceinline__ uint32_t lds32(const uint8_t* p, uint32_t o)
+__device__ __forceinline__ uint32_t lds32(saddr_t p, uint32_t o)
 {
     if constexpr (MODE == MODE_OUTLIER) {
-        const uint32_t* w = reinterpret_cast<const uint32_t*>(p + (o & ~3u));
+        const saddr_t w = p + (o & ~3u);
         const uint32_t sh = (o & 3u) * 8;
-        return sh ? __funnelshift_r(w[0], w[1], sh) : w[0];
+        const uint32_t lo = lds_u32(w);
+        return sh ? __funnelshift_r(lo, lds_u32(w + 4), sh) : lo;
     } else {
-        return *reinterpret_cast<const uint32_t*>(p + o);
+        return lds_u32(p + o);
     }
 }
 // Element 0's magnitude stored in `ob` (1..4) little-endian bytes at offset `o`: one
 // unaligned word read, masked (the bytes after it belong to the same payload).
-__device__ __forceinline__ uint32_t ld_outlier(const uint8_t* p, uint32_t o, uint32_t ob)
+__device__ __forceinline__ uint32_t ld_outlier(saddr_t p, uint32_t o, uint32_t ob)
 {
     const uint32_t w = lds32<MODE_OUTLIER>(p, o);
     return ob >= 4 ? w : w & ((1u << (8 * ob)) - 1u);
@@ -82,7 +83,7 @@ __device__ __forceinline__ uint32_t ld_outlier(const uint8_t* p, uint32_t o, uin
 // Decodes the 1D block pair (rates rA, rB at payload offsets oA, oB of `pay`) into the
 // codes of this lane's elements (dA, dB).
 template <int MODE>
-__device__ __forceinline__ void decode_pair_1d(const uint8_t* pay, uint32_t rA, uint32_t rB, uint32_t oA, uint32_t oB,
+__device__ __forceinline__ void decode_pair_1d(saddr_t pay, uint32_t rA, uint32_t rB, uint32_t oA, uint32_t oB,
                                                int32_t& dA, int32_t& dB, int lane)
 {
     uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
@@ -126,7 +127,7 @@ __device__ __forceinline__ void decode_pair_1d(const uint8_t* pay, uint32_t rA, 
 // Decodes one 2D/3D block (rate r at payload offset o) into the codes of this lane's
 // two elements (d0: element lane, d1: element lane + 32).
 template <int MODE>
-__device__ __forceinline__ void decode_block_nd(const uint8_t* pay, uint32_t r, uint32_t o, int32_t& d0, int32_t& d1,
+__device__ __forceinline__ void decode_block_nd(saddr_t pay, uint32_t r, uint32_t o, int32_t& d0, int32_t& d1,
                                                 int lane)
 {
     if (payload_size<2, MODE>(r) == 0) { d0 = 0; d1 = 0; return; }
@@ -159,7 +160,7 @@ __device__ __forceinline__ void decode_block_nd(const uint8_t* pay, uint32_t r, 
 // Two 2D/3D blocks at once: when both have payloads of rate <= 16 their transposes run
 // interleaved; otherwise one after the other.
 template <int MODE>
-__device__ __forceinline__ void decode_pair_nd(const uint8_t* pay, uint32_t ra, uint32_t rb, uint32_t oa, uint32_t ob_,
+__device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_t rb, uint32_t oa, uint32_t ob_,
                                                int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane)
 {
     uint32_t na = ra, nb = rb, oba = 0, obb = 0;
@@ -301,6 +302,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
     } else {
         // ---------------------------------------------------------------- codec warps
         T* ob = obuf + warp * (C::BPW * C::BLK);
+        const saddr_t obs = saddr(ob) + lane * (uint32_t)sizeof(T);   // this lane's element of block 0
         uint32_t parity = 0;      // bit f: phase parity of slot f's next fill
         uint32_t ended = 0;       // bit f: front warp f has no more tiles
         bool stored = false;      // this warp has bulk stores in flight
@@ -312,7 +314,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
             if (!mbar_wait(&sh.full[f], ph, err)) break;
             const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tile[f]);
             if ((uint64_t)t >= g.ntiles) { ended |= 1u << f; continue; }
-            const uint8_t* pay = slots + f * C::SLOT;
+            const saddr_t pay = saddr(slots + f * C::SLOT);
             const bool bad = sh.poff[f] == kBadSlot;
             // this warp's blocks: rate bytes, payload offsets (lane j: block j)
             const uint32_t myr = lane < C::BPW && !bad ? sh.rates[f][warp * C::BPW + lane] : 0u;
@@ -341,8 +343,8 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                         lorenzo_inverse<1>(dB, z, lane);
                     }
                     // blocks without payload decode to 0.0
-                    ob[j * 32 + lane] = payload_size<1, MODE>(rA) ? dequant(dA, eb) : T(0);
-                    ob[(j + 1) * 32 + lane] = payload_size<1, MODE>(rB) ? dequant(dB, eb) : T(0);
+                    sts_val(obs + j * 32 * sizeof(T), payload_size<1, MODE>(rA) ? dequant(dA, eb) : T(0));
+                    sts_val(obs + (j + 1) * 32 * sizeof(T), payload_size<1, MODE>(rB) ? dequant(dB, eb) : T(0));
                 }
             } else {
 #pragma unroll 1
@@ -356,10 +358,11 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                         lorenzo_inverse<DIM>(d0b, d1b, lane);
                     }
                     const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb) == 0;
-                    ob[j * 64 + lane] = za ? T(0) : dequant(d0a, eb);
-                    ob[j * 64 + 32 + lane] = za ? T(0) : dequant(d1a, eb);
-                    ob[j * 64 + 64 + lane] = zb ? T(0) : dequant(d0b, eb);
-                    ob[j * 64 + 96 + lane] = zb ? T(0) : dequant(d1b, eb);
+                    const saddr_t oj = obs + j * 64 * sizeof(T);
+                    sts_val(oj, za ? T(0) : dequant(d0a, eb));
+                    sts_val(oj + 32 * sizeof(T), za ? T(0) : dequant(d1a, eb));
+                    sts_val(oj + 64 * sizeof(T), zb ? T(0) : dequant(d0b, eb));
+                    sts_val(oj + 96 * sizeof(T), zb ? T(0) : dequant(d1b, eb));
                 }
             }
             __syncwarp();
