@@ -195,6 +195,46 @@ __device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, int
     }
 }
 
+// The per-lane constants of the five butterfly stages for a fixed row index, for loops
+// that transpose many words with the same row: keep mask and rotate amount per stage.
+struct XposeLane {
+    uint32_t keep[5];
+    uint32_t rot[5];
+    __device__ __forceinline__ explicit XposeLane(int row)
+    {
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            const int j = 16 >> i;
+            const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
+                             : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+            const bool up = row & j;
+            keep[i] = up ? m : ~m;
+            rot[i] = up ? (uint32_t)j : (uint32_t)(32 - j);
+        }
+    }
+};
+__device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, const XposeLane& xl)
+{
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        const int j = 16 >> i;
+        const uint32_t ya = __shfl_xor_sync(FULL, a, j);
+        const uint32_t yb = __shfl_xor_sync(FULL, b, j);
+        a = (a & xl.keep[i]) | (__funnelshift_r(ya, ya, xl.rot[i]) & ~xl.keep[i]);
+        b = (b & xl.keep[i]) | (__funnelshift_r(yb, yb, xl.rot[i]) & ~xl.keep[i]);
+    }
+}
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, const XposeLane& xl)
+{
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        const int j = 16 >> i;
+        const uint32_t y = __shfl_xor_sync(FULL, x, j);
+        x = (x & xl.keep[i]) | (__funnelshift_r(y, y, xl.rot[i]) & ~xl.keep[i]);
+    }
+    return x;
+}
+
 // Word with bit l = element l  <->  stored little-endian word whose byte b holds
 // elements 8b..8b+7 most-significant-bit first (the reference's plane/sign bytes).
 __device__ __forceinline__ uint32_t to_stream_word(uint32_t bits) { return __byte_perm(__brev(bits), 0, 0x0123); }

@@ -270,7 +270,7 @@ __device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lan
 // Payload of two 1D blocks A and B (rates rA, rB; codes cA, cB of this lane) at pA / pB.
 template <int MODE>
 __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t cA, int32_t cB, saddr_t pA,
-                                             saddr_t pB, int lane)
+                                             saddr_t pB, int lane, const XposeLane& xl)
 {
     uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -297,7 +297,7 @@ __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t c
         // (masks: a |INT_MIN| code, which the 1D rate ignores, must not reach the sign bits)
         const uint32_t x = (aA & 0x7fffu) | ((aB << 16) & 0x7fff0000u) | (((uint32_t)cA >> 16) & 0x8000u) |
                            ((uint32_t)cB & 0x80000000u);
-        const uint32_t y = warp_transpose32(x, lane ^ 7);
+        const uint32_t y = warp_transpose32(x, xl);
         const uint32_t p = (lane ^ 7) & 15;
         const bool b = lane >= 16;
         const uint32_t n = b ? nB : nA;
@@ -313,7 +313,7 @@ __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t c
         if (lane == 0 && hasA) put32s<MODE>(pA, sA);
         if (lane == 16 && hasB) put32s<MODE>(pB, sB);
         uint32_t yA = aA, yB = aB;
-        warp_transpose32x2(yA, yB, lane ^ 7);
+        warp_transpose32x2(yA, yB, xl);
         const int p = lane ^ 7;
         if ((uint32_t)p < nA) put32s<MODE>(pA + 4 + 4 * p, yA);
         if ((uint32_t)p < nB) put32s<MODE>(pB + 4 + 4 * p, yB);
@@ -322,7 +322,8 @@ __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t c
 
 // Payload of one 2D/3D block (rate r != 0; codes c0, c1 of this lane's two elements) at p.
 template <int MODE>
-__device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1, saddr_t p, int lane)
+__device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1, saddr_t p, int lane,
+                                              const XposeLane& xl)
 {
     uint32_t n = r, ob = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -342,7 +343,7 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
         // lane l holds plane (l ^ 7) & 15 of half l >> 4; plane 15 = the half's signs
         const uint32_t x = (a0 & 0x7fffu) | ((a1 << 16) & 0x7fff0000u) | (((uint32_t)c0 >> 16) & 0x8000u) |
                            ((uint32_t)c1 & 0x80000000u);
-        const uint32_t y = warp_transpose32(x, lane ^ 7);
+        const uint32_t y = warp_transpose32(x, xl);
         const uint32_t pl = (lane ^ 7) & 15;
         const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
         if (pl == 15) put32s<MODE>(p + h4, y);
@@ -352,7 +353,7 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
         const uint32_t s1 = to_stream_word(__ballot_sync(FULL, c1 < 0));
         if (lane < 2) put32s<MODE>(p + 4 * lane, lane ? s1 : s0);
         uint32_t ylo = a0, yhi = a1;
-        warp_transpose32x2(ylo, yhi, lane ^ 7);
+        warp_transpose32x2(ylo, yhi, xl);
         const int pl = lane ^ 7;
         if ((uint32_t)pl < n) {
             put32s<MODE>(p + 8 + 8 * pl, ylo);
@@ -365,7 +366,7 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
 // blocks' transposes run interleaved when both rates are <= 15.
 template <int MODE>
 __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c0a, int32_t c1a, int32_t c0b,
-                                             int32_t c1b, saddr_t pa, saddr_t pb, int lane)
+                                             int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
 {
     uint32_t na = ra, nb = rb, oba = 0, obb = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -374,8 +375,8 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
         if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
     }
     if (na > 15 || nb > 15) {
-        if (ra) pack_block_nd<MODE>(ra, c0a, c1a, pa, lane);
-        if (rb) pack_block_nd<MODE>(rb, c0b, c1b, pb, lane);
+        if (ra) pack_block_nd<MODE>(ra, c0a, c1a, pa, lane, xl);
+        if (rb) pack_block_nd<MODE>(rb, c0b, c1b, pb, lane, xl);
         return;
     }
     uint32_t a0a = uabs(c0a), a0b = uabs(c0b);
@@ -397,7 +398,7 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
                   ((uint32_t)c1a & 0x80000000u);
     uint32_t xb = (a0b & 0x7fffu) | ((a1b << 16) & 0x7fff0000u) | (((uint32_t)c0b >> 16) & 0x8000u) |
                   ((uint32_t)c1b & 0x80000000u);
-    warp_transpose32x2(xa, xb, lane ^ 7);
+    warp_transpose32x2(xa, xb, xl);
     const uint32_t pl = (lane ^ 7) & 15;
     const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
     const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
@@ -411,20 +412,22 @@ __device__ __forceinline__ void compress_pack(const CompressWork<T, DIM, Tl>& K,
 {
     constexpr int BPW = Tl::BPW;
     const int lane = threadIdx.x & 31;
+    const XposeLane xl(lane ^ 7);
     if constexpr (DIM == 1) {
 #pragma unroll
         for (int j = 0; j < BPW; j += 2) {
             const uint32_t rA = __shfl_sync(FULL, K.myrb, j), rB = __shfl_sync(FULL, K.myrb, j + 1);
             if ((rA | rB) == 0) continue;
             pack_pair_1d<MODE>(rA, rB, K.c0[j], K.c0[j + 1], saddr(pbase) + __shfl_sync(FULL, K.myoff, j),
-                               saddr(pbase) + __shfl_sync(FULL, K.myoff, j + 1), lane);
+                               saddr(pbase) + __shfl_sync(FULL, K.myoff, j + 1), lane, xl);
         }
     } else {
 #pragma unroll
         for (int j = 0; j < BPW; j++) {
             const uint32_t r = __shfl_sync(FULL, K.myrb, j);
             if (r == 0) continue;
-            pack_block_nd<MODE>(r, K.c0[j], K.c1[DIM == 1 ? 0 : j], saddr(pbase) + __shfl_sync(FULL, K.myoff, j), lane);
+            pack_block_nd<MODE>(r, K.c0[j], K.c1[DIM == 1 ? 0 : j], saddr(pbase) + __shfl_sync(FULL, K.myoff, j), lane,
+                                xl);
         }
     }
 }

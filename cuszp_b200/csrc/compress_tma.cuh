@@ -58,7 +58,8 @@ struct TmaCfg {
 
 // ------------------------------------------------------------------ mbarrier / TMA
 
-constexpr int kWaitLimit = 1 << 22;   // bounded mbarrier waits (with back-off: seconds)
+constexpr int kWaitLimit = 1 << 18;       // bounded mbarrier waits: attempts of up to kWaitSliceNs each
+constexpr uint32_t kWaitSliceNs = 8192;  // (so a wait gives up after about two seconds)
 enum : uint32_t { ERR_WAIT_TIMEOUT = 4u };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -88,6 +89,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity)
         : "memory");
     return ok != 0;
 }
+// try_wait with an explicit suspend-time hint: the warp sleeps in the barrier unit until
+// the phase completes (it then wakes at once) or `ns` nanoseconds pass -- waiting costs
+// no issue slots.
+__device__ __forceinline__ bool mbar_try_wait_ns(uint64_t* b, uint32_t parity, uint32_t ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
 // Non-blocking poll (try_wait may suspend the thread for a while before it fails).
 __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity)
 {
@@ -105,12 +121,9 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity)
 // did not within the limit.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint32_t* err)
 {
-    unsigned backoff = 32;
     for (int i = 0; i < kWaitLimit; i++) {
-        if (mbar_try_wait(b, parity)) return true;
-        if ((i & 1023) == 1023 && *reinterpret_cast<volatile uint32_t*>(err)) return false;   // another wait gave up
-        __nanosleep(backoff);
-        backoff = backoff < 512 ? 2 * backoff : 512;
+        if (mbar_try_wait_ns(b, parity, kWaitSliceNs)) return true;
+        if (*reinterpret_cast<volatile uint32_t*>(err)) return false;   // another wait gave up
     }
     atomicOr(err, ERR_WAIT_TIMEOUT);
     return false;
@@ -167,8 +180,7 @@ __device__ __forceinline__ uint32_t rate_pass_1d(saddr_t tin, saddr_t code, sadd
         const saddr_t wb = tin + (warp * C::BPW * 32 + lane) * (uint32_t)sizeof(T);
         const saddr_t wc = code + (warp * C::BPW * 32 + lane) * 4u;
         const bool ragged = (b0 + C::BPW) * 32 > g.nbEle;
-#pragma unroll 2
-        for (int j = 0; j < C::BPW; j += 2) {
+        auto step = [&](int j, bool mask) {
             const int32_t qA = quantize(lds_val<T>(wb + j * 32 * sizeof(T)), recip);
             const int32_t qB = quantize(lds_val<T>(wb + (j + 1) * 32 * sizeof(T)), recip);
             int32_t cA = qA, cB = qB;
@@ -177,7 +189,7 @@ __device__ __forceinline__ uint32_t rate_pass_1d(saddr_t tin, saddr_t code, sadd
                 cA = wsub(qA, lane ? uA : 0);
                 cB = wsub(qB, lane ? uB : 0);
             }
-            if (ragged) {
+            if (mask) {
                 const uint64_t i = (b0 + j) * 32 + lane;
                 cA = i < g.nbEle ? cA : 0;
                 cB = i + 32 < g.nbEle ? cB : 0;
@@ -189,6 +201,13 @@ __device__ __forceinline__ uint32_t rate_pass_1d(saddr_t tin, saddr_t code, sadd
             if (lane == j) rb = rA;
             if (lane == j + 1) rb = rB;
             off += payload_size<1, MODE>(rA) + payload_size<1, MODE>(rB);
+        };
+        if (ragged) {
+#pragma unroll 1
+            for (int j = 0; j < C::BPW; j += 2) step(j, true);
+        } else {
+#pragma unroll 4
+            for (int j = 0; j < C::BPW; j += 2) step(j, false);
         }
     }
     if (lane < C::BPW) {
@@ -250,6 +269,38 @@ __device__ __forceinline__ uint32_t rate_pass_nd(saddr_t tin, saddr_t code, sadd
                 c1 = ok1 ? c1 : 0;
             }
         };
+        if (!ragged && nblk == C::BPW) {
+            // every block whole: no masks, four independent blocks per step
+#pragma unroll
+            for (int j = 0; j < C::BPW; j += 4) {
+                int32_t c0[4], c1[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const saddr_t blk = wb + (j + u) * 64 * sizeof(T);
+                    const int32_t q0 = quantize(lds_val<T>(blk), recip);
+                    const int32_t q1 = quantize(lds_val<T>(blk + 32 * sizeof(T)), recip);
+                    c0[u] = q0;
+                    c1[u] = q1;
+                    if constexpr (MODE != MODE_FIXED) {
+                        int32_t p0, p1;
+                        predecessors<DIM>(q0, q1, lane, p0, p1);
+                        c0[u] = wsub(q0, p0);
+                        c1[u] = wsub(q1, p1);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    sts_u32(wc + (j + u) * 256, (uint32_t)c0[u]);
+                    sts_u32(wc + (j + u) * 256 + 128, (uint32_t)c1[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const uint32_t r = block_rate<DIM, MODE>(uabs(c0[u]), uabs(c1[u]), lane);
+                    if (lane == j + u) rbyte = r;
+                    off += payload_size<DIM, MODE>(r);
+                }
+            }
+        } else {
 #pragma unroll 1
         for (uint32_t j = 0; j < nblk; j += 2) {
             uint32_t xb2 = bx, yb2 = by, zb2 = bz;
@@ -271,6 +322,7 @@ __device__ __forceinline__ uint32_t rate_pass_nd(saddr_t tin, saddr_t code, sadd
             bx = xb2; by = yb2; bz = zb2;
             advance(bx, by, bz);
         }
+        }
     }
     if (lane < C::BPW) {
         sts_u8(rates + warp * C::BPW + lane, rbyte);
@@ -288,6 +340,7 @@ __device__ __forceinline__ uint32_t pack_pass(saddr_t code, saddr_t rates, int w
 {
     const saddr_t wc = code + (warp * C::BPW * C::BLK + lane) * 4u;   // this lane's code of block 0
     const uint32_t mine = lane < C::BPW ? lds_u8(rates + warp * C::BPW + lane) : 0u;
+    const XposeLane xl(lane ^ 7);
     uint32_t off = 0;
 #pragma unroll 1
     for (int j = 0; j < C::BPW; j += 2) {
@@ -296,11 +349,11 @@ __device__ __forceinline__ uint32_t pack_pass(saddr_t code, saddr_t rates, int w
         if (ra | rb) {
             if constexpr (DIM == 1) {
                 pack_pair_1d<MODE>(ra, rb, (int32_t)lds_u32(wc + j * 128), (int32_t)lds_u32(wc + (j + 1) * 128),
-                                   region + off, region + off + sa, lane);
+                                   region + off, region + off + sa, lane, xl);
             } else {
                 const saddr_t ca = wc + j * 256;
                 pack_pair_nd<MODE>(ra, rb, (int32_t)lds_u32(ca), (int32_t)lds_u32(ca + 128), (int32_t)lds_u32(ca + 256),
-                                   (int32_t)lds_u32(ca + 384), region + off, region + off + sa, lane);
+                                   (int32_t)lds_u32(ca + 384), region + off, region + off + sa, lane, xl);
             }
         }
         off += sa + payload_size<DIM, MODE>(rb);
@@ -382,13 +435,10 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
             const int c = k % C::NC;
             const uint32_t parity = (uint32_t)(k / C::NC) & 1u;
             bool ready = false;
-            unsigned backoff = 32;
-            for (int i = 0; i < kWaitLimit; i++) {   // tile k's rate pass done, or no tile k
-                if (mbar_try_wait(&sh.aggd[c], parity)) { ready = true; break; }
+            for (int i = 0; i < 4 * kWaitLimit; i++) {   // tile k's rate pass done, or no tile k
+                if (mbar_try_wait_ns(&sh.aggd[c], parity, kWaitSliceNs / 4)) { ready = true; break; }
                 if (k >= *reinterpret_cast<volatile int*>(&sh.kend)) break;
-                if ((i & 1023) == 1023 && *reinterpret_cast<volatile uint32_t*>(err)) break;
-                __nanosleep(backoff);
-                backoff = backoff < 512 ? 2 * backoff : 512;
+                if (*reinterpret_cast<volatile uint32_t*>(err)) break;
             }
             if (!ready) break;
             const int64_t t = sh.tile_of[c];

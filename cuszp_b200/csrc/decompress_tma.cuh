@@ -84,7 +84,7 @@ __device__ __forceinline__ uint32_t ld_outlier(saddr_t p, uint32_t o, uint32_t o
 // codes of this lane's elements (dA, dB).
 template <int MODE>
 __device__ __forceinline__ void decode_pair_1d(saddr_t pay, uint32_t rA, uint32_t rB, uint32_t oA, uint32_t oB,
-                                               int32_t& dA, int32_t& dB, int lane)
+                                               int32_t& dA, int32_t& dB, int lane, const XposeLane& xl)
 {
     uint32_t nA = rA, nB = rB, obA = 0, obB = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -101,7 +101,7 @@ __device__ __forceinline__ void decode_pair_1d(saddr_t pay, uint32_t rA, uint32_
         if (lane < 16) { if (p < nA) w = lds32<MODE>(pay, pA + 4 + 4 * p); }
         else           { if (p < nB) w = lds32<MODE>(pay, pB + 4 + 4 * p); }
         if (nA | nB) {
-            const uint32_t x = warp_transpose32(from_stream_word(w), lane);
+            const uint32_t x = warp_transpose32(from_stream_word(w), xl);
             magA = x & 0xffffu;
             magB = x >> 16;
         }
@@ -110,7 +110,7 @@ __device__ __forceinline__ void decode_pair_1d(saddr_t pay, uint32_t rA, uint32_
         const uint32_t wB = (uint32_t)lane < nB ? lds32<MODE>(pay, pB + 4 + 4 * lane) : 0u;
         magA = from_stream_word(wA);
         magB = from_stream_word(wB);
-        warp_transpose32x2(magA, magB, lane);
+        warp_transpose32x2(magA, magB, xl);
     }
     if constexpr (MODE == MODE_OUTLIER) {
         if (lane == 0) {
@@ -128,7 +128,7 @@ __device__ __forceinline__ void decode_pair_1d(saddr_t pay, uint32_t rA, uint32_
 // two elements (d0: element lane, d1: element lane + 32).
 template <int MODE>
 __device__ __forceinline__ void decode_block_nd(saddr_t pay, uint32_t r, uint32_t o, int32_t& d0, int32_t& d1,
-                                                int lane)
+                                                int lane, const XposeLane& xl)
 {
     if (payload_size<2, MODE>(r) == 0) { d0 = 0; d1 = 0; return; }
     uint32_t n = r, ob = 0;
@@ -141,13 +141,13 @@ __device__ __forceinline__ void decode_block_nd(saddr_t pay, uint32_t r, uint32_
     if (n <= 16) {
         const uint32_t pl = lane & 15;
         const uint32_t w = pl < n ? lds32<MODE>(pay, p + 8 + 8 * pl + (lane >> 4) * 4) : 0u;
-        const uint32_t x = warp_transpose32(from_stream_word(w), lane);
+        const uint32_t x = warp_transpose32(from_stream_word(w), xl);
         mag0 = x & 0xffffu;
         mag1 = x >> 16;
     } else {
         mag0 = (uint32_t)lane < n ? from_stream_word(lds32<MODE>(pay, p + 8 + 8 * lane)) : 0u;
         mag1 = (uint32_t)lane < n ? from_stream_word(lds32<MODE>(pay, p + 12 + 8 * lane)) : 0u;
-        warp_transpose32x2(mag0, mag1, lane);
+        warp_transpose32x2(mag0, mag1, xl);
     }
     if constexpr (MODE == MODE_OUTLIER) {
         if (ob && lane == 0) mag0 = ld_outlier(pay, o, ob);
@@ -161,7 +161,8 @@ __device__ __forceinline__ void decode_block_nd(saddr_t pay, uint32_t r, uint32_
 // interleaved; otherwise one after the other.
 template <int MODE>
 __device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_t rb, uint32_t oa, uint32_t ob_,
-                                               int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane)
+                                               int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane,
+                                               const XposeLane& xl)
 {
     uint32_t na = ra, nb = rb, oba = 0, obb = 0;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -170,8 +171,8 @@ __device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_
         if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
     }
     if (na > 16 || nb > 16 || payload_size<2, MODE>(ra) == 0 || payload_size<2, MODE>(rb) == 0) {
-        decode_block_nd<MODE>(pay, ra, oa, d0a, d1a, lane);
-        decode_block_nd<MODE>(pay, rb, ob_, d0b, d1b, lane);
+        decode_block_nd<MODE>(pay, ra, oa, d0a, d1a, lane, xl);
+        decode_block_nd<MODE>(pay, rb, ob_, d0b, d1b, lane, xl);
         return;
     }
     const uint32_t pa = oa + oba, pb = ob_ + obb;   // sign words
@@ -180,7 +181,7 @@ __device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_
     uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : 0u;
     xa = from_stream_word(xa);
     xb = from_stream_word(xb);
-    warp_transpose32x2(xa, xb, lane);
+    warp_transpose32x2(xa, xb, xl);
     uint32_t m0a = xa & 0xffffu, m1a = xa >> 16, m0b = xb & 0xffffu, m1b = xb >> 16;
     if constexpr (MODE == MODE_OUTLIER) {
         if (lane == 0) {
@@ -303,6 +304,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
         // ---------------------------------------------------------------- codec warps
         T* ob = obuf + warp * (C::BPW * C::BLK);
         const saddr_t obs = saddr(ob) + lane * (uint32_t)sizeof(T);   // this lane's element of block 0
+        const XposeLane xl(lane);
         uint32_t parity = 0;      // bit f: phase parity of slot f's next fill
         uint32_t ended = 0;       // bit f: front warp f has no more tiles
         bool stored = false;      // this warp has bulk stores in flight
@@ -336,7 +338,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                     const uint32_t rA = __shfl_sync(FULL, myr, j), rB = __shfl_sync(FULL, myr, j + 1);
                     const uint32_t oA = __shfl_sync(FULL, myo, j), oB = __shfl_sync(FULL, myo, j + 1);
                     int32_t dA, dB;
-                    decode_pair_1d<MODE>(pay, rA, rB, oA, oB, dA, dB, lane);
+                    decode_pair_1d<MODE>(pay, rA, rB, oA, oB, dA, dB, lane, xl);
                     if constexpr (MODE != MODE_FIXED) {
                         int32_t z = 0;
                         lorenzo_inverse<1>(dA, z, lane);
@@ -352,7 +354,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                     const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
                     const uint32_t rb = __shfl_sync(FULL, myr, j + 1), obo = __shfl_sync(FULL, myo, j + 1);
                     int32_t d0a, d1a, d0b, d1b;
-                    decode_pair_nd<MODE>(pay, ra, rb, oa, obo, d0a, d1a, d0b, d1b, lane);
+                    decode_pair_nd<MODE>(pay, ra, rb, oa, obo, d0a, d1a, d0b, d1b, lane, xl);
                     if constexpr (MODE != MODE_FIXED) {
                         lorenzo_inverse<DIM>(d0a, d1a, lane);
                         lorenzo_inverse<DIM>(d0b, d1b, lane);
