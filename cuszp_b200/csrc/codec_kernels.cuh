@@ -362,9 +362,10 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
     }
 }
 
-// Payloads of two 2D/3D blocks a and b (rates ra, rb, not both 0) at pa / pb; both
-// blocks' transposes run interleaved when both rates are <= 15.
-template <int MODE>
+// Payloads of two 2D/3D blocks a and b (rates ra, rb) at pa / pb; both blocks'
+// transposes run interleaved when both rates are <= 15.  NARROW: the caller knows
+// both rates are <= 15 (no fallback branch, so consecutive pairs can interleave).
+template <int MODE, bool NARROW = false>
 __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c0a, int32_t c1a, int32_t c0b,
                                              int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
 {
@@ -374,7 +375,7 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
         if (ra & 0x80) oba = ((ra & 0x60) >> 5) + 1;
         if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
     }
-    if (na > 15 || nb > 15) {
+    if (!NARROW && (na > 15 || nb > 15)) {
         if (ra) pack_block_nd<MODE>(ra, c0a, c1a, pa, lane, xl);
         if (rb) pack_block_nd<MODE>(rb, c0b, c1b, pb, lane, xl);
         return;

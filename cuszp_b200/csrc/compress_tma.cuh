@@ -341,6 +341,30 @@ __device__ __forceinline__ uint32_t pack_pass(saddr_t code, saddr_t rates, int w
     const saddr_t wc = code + (warp * C::BPW * C::BLK + lane) * 4u;   // this lane's code of block 0
     const uint32_t mine = lane < C::BPW ? lds_u8(rates + warp * C::BPW + lane) : 0u;
     const XposeLane xl(lane ^ 7);
+    if constexpr (DIM != 1) {
+        const uint32_t n = MODE == MODE_OUTLIER ? (mine & 0x1fu) : mine;
+        if (__all_sync(FULL, n <= 15)) {
+            // every block narrow: offsets up front, all pairs unrolled (no branches between)
+            const uint32_t sz = payload_size<DIM, MODE>(mine);
+            uint32_t incl = sz;
+#pragma unroll
+            for (int o = 1; o < C::BPW; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t myoff = incl - sz;
+#pragma unroll
+            for (int j = 0; j < C::BPW; j += 2) {
+                const uint32_t ra = __shfl_sync(FULL, mine, j), rb = __shfl_sync(FULL, mine, j + 1);
+                const uint32_t oa = __shfl_sync(FULL, myoff, j), ob = __shfl_sync(FULL, myoff, j + 1);
+                const saddr_t ca = wc + j * 256;
+                pack_pair_nd<MODE, true>(ra, rb, (int32_t)lds_u32(ca), (int32_t)lds_u32(ca + 128),
+                                         (int32_t)lds_u32(ca + 256), (int32_t)lds_u32(ca + 384), region + oa,
+                                         region + ob, lane, xl);
+            }
+            return __shfl_sync(FULL, incl, C::BPW - 1);
+        }
+    }
     uint32_t off = 0;
 #pragma unroll 1
     for (int j = 0; j < C::BPW; j += 2) {
