@@ -48,6 +48,30 @@ struct WsHeader {
 };
 static_assert(sizeof(WsHeader) == 48, "header layout");
 
+// Unsigned 32-bit division by an invariant divisor d >= 1 as a multiply-high and shifts
+// (Granlund & Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> 1)) >> (l - 1), t = umulhi(m, n); d == 1 is n itself.
+struct FastDiv {
+    uint32_t m, s1, s2;   // multiplier and the two shifts (s1 = 1, s2 = l - 1; both 0 for d == 1)
+    __host__ __device__ static FastDiv make(uint32_t d)
+    {
+        FastDiv f{0u, 0u, 0u};
+        if (d <= 1) return f;
+        uint32_t l = 0;
+        while (l < 32 && (1ull << l) < d) l++;
+        f.m = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+        f.s1 = 1;
+        f.s2 = l - 1;
+        return f;
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const
+    {
+        const uint32_t t = __umulhi(m, n);
+        return (t + ((n - t) >> s1)) >> s2;
+    }
+};
+
 struct Geom {
     uint64_t nbEle;        // 1D element count
     uint32_t dx, dy, dz;   // dims.x fastest
@@ -55,6 +79,8 @@ struct Geom {
     uint64_t nblocks;      // data blocks that exist
     uint64_t rate_bytes;   // size of the rate region
     uint64_t ntiles;       // tiles handed out (1D: covers the whole rate region)
+    FastDiv div_bx;        // division by bxn
+    FastDiv div_plane;     // division by bxn * byn
 };
 
 // ------------------------------------------------------------------ scalar helpers

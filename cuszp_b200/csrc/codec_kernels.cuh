@@ -76,9 +76,9 @@ __device__ __forceinline__ BlockPos block_pos(uint64_t b, const Geom& g)
     const uint32_t per = g.bxn * g.byn;
     const uint32_t bb = (uint32_t)b;
     BlockPos p;
-    p.z = bb / per;
+    p.z = g.div_plane.div(bb);
     const uint32_t r = bb - p.z * per;
-    p.y = r / g.bxn;
+    p.y = g.div_bx.div(r);
     p.x = r - p.y * g.bxn;
     return p;
 }

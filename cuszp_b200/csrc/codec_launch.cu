@@ -34,6 +34,9 @@ int make_problem(Problem& p, int type, int mode, int dim, size_t nbEle, unsigned
         g.byn = (uint32_t)((dy + bs - 1) / bs);
         const uint64_t nbz = dim == 2 ? dz : (dz + 3) / 4;
         g.nblocks = nbz * g.byn * g.bxn;
+        if ((uint64_t)g.bxn * g.byn > 0xffffffffull) return E_ARG;
+        g.div_bx = FastDiv::make(g.bxn);
+        g.div_plane = FastDiv::make(g.bxn * g.byn);
         if (g.nblocks > 0xffffffffull) return E_ARG;
         g.rate_bytes = (g.nblocks + 3) / 4 * 4;
         g.ntiles = (g.nblocks + Tiling<2>::TB - 1) / Tiling<2>::TB;
