@@ -35,6 +35,9 @@ lib.cuSZp_batch_plan_set_config.restype = ctypes.c_int
 lib.cuSZp_batch_plan_config.argtypes = [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]
 lib.cuSZp_batch_plan_config.restype = ctypes.c_int
+lib.cuSZp_batch_plan_variant.argtypes = [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int)]
+lib.cuSZp_batch_plan_variant.restype = ctypes.c_int
 lib.cuSZp_batch_plan_eb.argtypes = [_P, ctypes.POINTER(ctypes.c_float), _P]
 lib.cuSZp_batch_plan_eb.restype = ctypes.c_int
 lib.cuSZp_batch_plan_check.argtypes = [_P, _P]
@@ -96,10 +99,16 @@ class BatchPlan:
         _check(lib.cuSZp_batch_plan_set_config(self.handle, variant, ctas_per_sm), "batch config")
 
     def config(self):
+        """Kernel pair in use: variant index (0 = the TMA pair), codec warps, blocks per
+        codec warp, CTAs per SM (0 = occupancy limit) and threads per CTA."""
         w, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        lib.cuSZp_batch_plan_config(self.handle, ctypes.byref(w), ctypes.byref(b), ctypes.byref(c))
-        return {"warps": w.value, "blocks_per_warp": b.value, "ctas_per_sm": c.value,
-                "threads_per_block": 32 * w.value}
+        _check(lib.cuSZp_batch_plan_config(self.handle, ctypes.byref(w), ctypes.byref(b), ctypes.byref(c)),
+               "batch config")
+        v, t, tma = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib.cuSZp_batch_plan_variant(self.handle, ctypes.byref(v), ctypes.byref(t), ctypes.byref(tma)),
+               "batch variant")
+        return {"variant": v.value, "tma": bool(tma.value), "warps": w.value, "blocks_per_warp": b.value,
+                "ctas_per_sm": c.value, "threads_per_block": t.value}
 
     def check(self, stream=None):
         s = stream if stream is not None else torch.cuda.current_stream()

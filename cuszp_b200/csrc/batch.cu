@@ -11,6 +11,7 @@
 #include "batch.cuh"
 #include "codec_kernels.cuh"
 #include "codec_launch.cuh"
+#include "decompress_tma.cuh"
 
 #include <algorithm>
 #include <type_traits>
@@ -227,12 +228,73 @@ decompress_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __r
     finish_cta(hdr, status, total_tiles);
 }
 
+// ------------------------------------------------------------------ batched TMA codec
+
+// Tile source of the warp-specialised TMA kernels over the arrays of a batch: the tile
+// map names a global tile's array; each array has its own stream, status words, bound,
+// encoding mode and (2D/3D) tensor map.  COMP: items hold (data, stream), else
+// (stream, data).
+template <typename T, bool COMP>
+struct BatchTiles {
+    const BatchItem* items;
+    const uint32_t* tile_map;
+    const CUtensorMap* tmaps;   // one per array (2D/3D); written by the host before the launch
+    uint64_t total_tiles;
+    unsigned long long* status;
+    unsigned long long* sizes;
+    __device__ __forceinline__ uint64_t total() const { return total_tiles; }
+    __device__ __forceinline__ void locate(int64_t t, int32_t& a, int64_t& local) const
+    {
+        a = (int32_t)__ldg(tile_map + t);
+        local = t - (int64_t)items[a].tile_start;
+    }
+    __device__ __forceinline__ TileArray array(int32_t a) const
+    {
+        const BatchItem& it = items[a];
+        void* data = COMP ? const_cast<void*>(it.in) : it.out;
+        uint8_t* cmp = static_cast<uint8_t*>(COMP ? it.out : const_cast<void*>(it.in));
+        return TileArray{data, cmp, &it.g, status + it.tile_start, sizes + a, tmaps + a, it.eb, it.mode};
+    }
+    __device__ __forceinline__ T recip_of(const TileArray& A) const { return cuszp::recip_of<T>(A.eb); }
+    __device__ __forceinline__ T eb_of(const TileArray& A) const { return (T)A.eb; }
+    // The map was copied into global memory by the host: order that write before the
+    // tensor-map proxy reads it.
+    __device__ __forceinline__ void acquire_map(const CUtensorMap* m) const
+    {
+        asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(m) : "memory");
+    }
+    template <typename F>
+    __device__ __forceinline__ void with_mode(int mode, F&& f) const { cuszp::with_mode(mode, static_cast<F&&>(f)); }
+};
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(TmaCfg<T, DIM>::THREADS, 2)
+compress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
+                          const CUtensorMap* __restrict__ tmaps, uint64_t total_tiles, WsHeader* __restrict__ hdr,
+                          unsigned long long* __restrict__ status, unsigned long long* __restrict__ sizes)
+{
+    const BatchTiles<T, true> src{items, tile_map, tmaps, total_tiles, status, sizes};
+    compress_tma_body<T, DIM>(src, hdr, status);
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
+decompress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
+                            const CUtensorMap* __restrict__ tmaps, uint64_t total_tiles, WsHeader* __restrict__ hdr,
+                            unsigned long long* __restrict__ status, unsigned long long* __restrict__ sizes)
+{
+    const BatchTiles<T, false> src{items, tile_map, tmaps, total_tiles, status, sizes};
+    decompress_tma_body<T, DIM>(src, hdr, status);
+}
+
 // ------------------------------------------------------------------ tile-shape variants
 
 struct Variant {
-    int warps, bpw1, bpwn;   // warps per CTA; data blocks per warp in 1D and in 2D/3D
+    int warps, bpw1, bpwn;   // codec warps per CTA; data blocks per codec warp in 1D and in 2D/3D
+    int threads;             // threads per CTA
+    bool tma;                // warp-specialised TMA kernels: arrays on 16-byte boundaries only
     const void* (*kernel)(int type, int dim, bool comp);
-    size_t (*smem)(int type, int dim);   // dynamic shared memory of the compress kernel
+    size_t (*smem)(int type, int dim, bool comp);   // dynamic shared memory (set on first use)
 };
 
 template <int DIM, int WARPS, int BPW>
@@ -243,20 +305,24 @@ static const void* kernel_for_variant(int type, bool comp)
     return comp ? (const void*)compress_batch_kernel<double, DIM, Tl> : (const void*)decompress_batch_kernel<double, DIM, Tl>;
 }
 
-// Looks up (and on first use enables) the dynamic shared memory of a compress kernel.
-template <typename T, int DIM, typename Tl>
-static size_t smem_for_variant()
+// Enables (once per device) the dynamic shared memory a kernel needs and returns it.
+static size_t enable_smem(const void* fn, size_t bytes, bool* set)
 {
-    static bool set[64] = {};   // the attribute is per device
-    constexpr size_t bytes = compress_smem_bytes<T, DIM, Tl>();
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !set[dev]) {
-        cudaFuncSetAttribute((const void*)compress_batch_kernel<T, DIM, Tl>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         set[dev] = true;
     }
     return bytes;
+}
+
+template <typename T, int DIM, typename Tl>
+static size_t smem_for_variant(bool comp)
+{
+    static bool set[64] = {};   // the attribute is per device
+    if (!comp) return 0;
+    return enable_smem((const void*)compress_batch_kernel<T, DIM, Tl>, compress_smem_bytes<T, DIM, Tl>(), set);
 }
 
 template <int WARPS, int BPW1D, int BPWND>
@@ -268,25 +334,57 @@ static const void* kv(int type, int dim, bool comp)
 }
 
 template <int WARPS, int BPW1D, int BPWND>
-static size_t ks(int type, int dim)
+static size_t ks(int type, int dim, bool comp)
 {
     if (type == 0) {
-        if (dim == 1) return smem_for_variant<float, 1, Tiling<1, WARPS, BPW1D>>();
-        if (dim == 2) return smem_for_variant<float, 2, Tiling<2, WARPS, BPWND>>();
-        return smem_for_variant<float, 3, Tiling<3, WARPS, BPWND>>();
+        if (dim == 1) return smem_for_variant<float, 1, Tiling<1, WARPS, BPW1D>>(comp);
+        if (dim == 2) return smem_for_variant<float, 2, Tiling<2, WARPS, BPWND>>(comp);
+        return smem_for_variant<float, 3, Tiling<3, WARPS, BPWND>>(comp);
     }
-    if (dim == 1) return smem_for_variant<double, 1, Tiling<1, WARPS, BPW1D>>();
-    if (dim == 2) return smem_for_variant<double, 2, Tiling<2, WARPS, BPWND>>();
-    return smem_for_variant<double, 3, Tiling<3, WARPS, BPWND>>();
+    if (dim == 1) return smem_for_variant<double, 1, Tiling<1, WARPS, BPW1D>>(comp);
+    if (dim == 2) return smem_for_variant<double, 2, Tiling<2, WARPS, BPWND>>(comp);
+    return smem_for_variant<double, 3, Tiling<3, WARPS, BPWND>>(comp);
 }
 
-// (warps per CTA, blocks per warp in 1D, blocks per warp in 2D/3D)
+template <typename T, int DIM>
+static const void* tma_batch_kernel(bool comp)
+{
+    return comp ? (const void*)compress_tma_batch_kernel<T, DIM> : (const void*)decompress_tma_batch_kernel<T, DIM>;
+}
+
+template <typename T, int DIM>
+static size_t tma_batch_smem(bool comp)
+{
+    static bool set[2][64] = {};
+    return comp ? enable_smem(tma_batch_kernel<T, DIM>(true), TmaCfg<T, DIM>::smem_bytes(), set[0])
+                : enable_smem(tma_batch_kernel<T, DIM>(false), DecCfg<T, DIM>::smem_bytes(), set[1]);
+}
+
+static const void* tk(int type, int dim, bool comp)
+{
+    if (type == 0) return dim == 1 ? tma_batch_kernel<float, 1>(comp) : dim == 2 ? tma_batch_kernel<float, 2>(comp) : tma_batch_kernel<float, 3>(comp);
+    return dim == 1 ? tma_batch_kernel<double, 1>(comp) : dim == 2 ? tma_batch_kernel<double, 2>(comp) : tma_batch_kernel<double, 3>(comp);
+}
+
+static size_t tks(int type, int dim, bool comp)
+{
+    if (type == 0) return dim == 1 ? tma_batch_smem<float, 1>(comp) : dim == 2 ? tma_batch_smem<float, 2>(comp) : tma_batch_smem<float, 3>(comp);
+    return dim == 1 ? tma_batch_smem<double, 1>(comp) : dim == 2 ? tma_batch_smem<double, 2>(comp) : tma_batch_smem<double, 3>(comp);
+}
+
+// Variant 0 is the TMA kernel pair (8 codec warps; the same tiles as variant 1);
+// then the cp.async kernels as (warps per CTA, blocks per warp in 1D, in 2D/3D).
 static const Variant kVariants[] = {
-    {8, 16, 8, kv<8, 16, 8>, ks<8, 16, 8>},
-    {4, 16, 8, kv<4, 16, 8>, ks<4, 16, 8>},
-    {8, 8, 4, kv<8, 8, 4>, ks<8, 8, 4>},
-    {16, 8, 4, kv<16, 8, 4>, ks<16, 8, 4>},
+    {8, 16, 8, TmaCfg<float, 1>::THREADS, true, tk, tks},
+    {8, 16, 8, 256, false, kv<8, 16, 8>, ks<8, 16, 8>},
+    {4, 16, 8, 128, false, kv<4, 16, 8>, ks<4, 16, 8>},
+    {8, 8, 4, 256, false, kv<8, 8, 4>, ks<8, 8, 4>},
+    {16, 8, 4, 512, false, kv<16, 8, 4>, ks<16, 8, 4>},
 };
+static_assert(TmaCfg<float, 1>::THREADS == TmaCfg<double, 3>::THREADS &&
+                  DecCfg<float, 1>::THREADS == TmaCfg<float, 1>::THREADS,
+              "one thread count for every TMA batch kernel");
+static_assert(TmaCfg<float, 1>::TB == 8 * 16 && TmaCfg<float, 2>::TB == 8 * 8, "TMA tiles as in variant 1");
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 }  // namespace cuszp
@@ -298,8 +396,10 @@ struct cuszp_batch_plan {
     int dim = 1, type = 0;
     bool compress = true;
     bool any_rel = false;
-    int variant = 0;
+    int variant = 1;
     int ctas_per_sm = 0;       // 0: occupancy limit
+    bool tma_ok = false;       // every array suits the TMA kernels (variant 0)
+    CUtensorMap* d_maps = nullptr;   // per-array tensor maps of the TMA kernels (2D/3D)
     int sms = 148;
     std::vector<cuszp_batch_item_t> host_items;
     std::vector<BatchItem> items;
@@ -366,6 +466,34 @@ static int plan_layout(cuszp_batch_plan* p, int variant, cudaStream_t s)
     return OK;
 }
 
+// Decides whether every array suits the TMA kernels (data and stream on 16-byte
+// boundaries; for 2D/3D a tensor map the driver accepts) and uploads the maps.
+static int plan_maps(cuszp_batch_plan* p, cudaStream_t s)
+{
+    p->tma_ok = tma_allowed();
+    std::vector<CUtensorMap> maps(p->dim == 1 ? 0 : (size_t)p->count);
+    for (int a = 0; a < p->count && p->tma_ok; a++) {
+        const cuszp_batch_item_t& h = p->host_items[a];
+        if (h.nbEle == 0) continue;   // no tiles
+        if ((reinterpret_cast<uintptr_t>(h.d_in) | reinterpret_cast<uintptr_t>(h.d_out)) & 15u) p->tma_ok = false;
+        if (p->dim == 1 || !p->tma_ok) continue;
+        Problem pr;
+        if (make_problem(pr, p->type, h.mode, p->dim, h.nbEle, h.dims.x, h.dims.y, h.dims.z)) {
+            p->tma_ok = false;
+            continue;
+        }
+        std::memset(&maps[a], 0, sizeof(CUtensorMap));
+        if (!make_block_map(&maps[a], pr, p->compress ? h.d_in : h.d_out)) p->tma_ok = false;
+    }
+    if (!p->tma_ok || maps.empty()) return OK;
+    if (cudaMallocAsync((void**)&p->d_maps, sizeof(CUtensorMap) * maps.size(), s) != cudaSuccess) return E_CUDA;
+    // pageable source: staged before the call returns
+    if (cudaMemcpyAsync(p->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, s) !=
+        cudaSuccess)
+        return E_CUDA;
+    return OK;
+}
+
 static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStream_t s)
 {
     char* ws = static_cast<char*>(p->d_ws);
@@ -384,9 +512,9 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     if (p->total_tiles == 0) return cudaGetLastError() == cudaSuccess ? OK : E_CUDA;
     const Variant& v = kVariants[p->variant];
     const void* fn = v.kernel(p->type, p->dim, p->compress);
-    const size_t smem = p->compress ? v.smem(p->type, p->dim) : 0;
+    const size_t smem = v.smem(p->type, p->dim, p->compress);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.warps * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.threads, smem);
     if (occ < 1) occ = 1;
     const int per_sm = p->ctas_per_sm > 0 ? std::min(p->ctas_per_sm, occ) : occ;
     const uint64_t want = (uint64_t)p->sms * per_sm;
@@ -396,8 +524,13 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     uint64_t total = p->total_tiles;
     WsHeader* hdr = (WsHeader*)ws;
     unsigned long long* status = (unsigned long long*)(ws + p->status_off);
-    void* args[] = {(void*)&items, (void*)&map, (void*)&total, (void*)&hdr, (void*)&status, (void*)&d_sizes};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(v.warps * 32), args, smem, s) == cudaSuccess ? OK : E_CUDA;
+    const CUtensorMap* maps = p->d_maps;
+    void* args_cp[] = {(void*)&items, (void*)&map, (void*)&total, (void*)&hdr, (void*)&status, (void*)&d_sizes};
+    void* args_tma[] = {(void*)&items, (void*)&map, (void*)&maps, (void*)&total, (void*)&hdr, (void*)&status,
+                        (void*)&d_sizes};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(v.threads), v.tma ? args_tma : args_cp, smem, s) == cudaSuccess
+               ? OK
+               : E_CUDA;
 }
 
 extern "C" int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
@@ -426,10 +559,12 @@ extern "C" int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count
         delete p;
         return E_CUDA;
     }
-    const int st = plan_layout(p, 0, stream);
+    int st = plan_maps(p, stream);
+    if (!st) st = plan_layout(p, p->tma_ok ? 0 : 1, stream);
     if (st) {
         cudaFreeAsync(p->d_items, stream);
         if (p->d_ws) cudaFreeAsync(p->d_ws, stream);
+        if (p->d_maps) cudaFreeAsync(p->d_maps, stream);
         delete p;
         return st;
     }
@@ -457,6 +592,15 @@ extern "C" int cuSZp_batch_plan_check(cuszp_batch_plan_t p, cudaStream_t stream)
     return cuSZp_workspace_check(p->d_ws, p->ws_bytes, stream);
 }
 
+extern "C" int cuSZp_batch_plan_variant(cuszp_batch_plan_t p, int* variant, int* threadsPerBlock, int* tma)
+{
+    if (!p) return E_ARG;
+    if (variant) *variant = p->variant;
+    if (threadsPerBlock) *threadsPerBlock = kVariants[p->variant].threads;
+    if (tma) *tma = kVariants[p->variant].tma ? 1 : 0;
+    return OK;
+}
+
 extern "C" int cuSZp_batch_plan_config(cuszp_batch_plan_t p, int* warps, int* blocks_per_warp, int* ctas_per_sm)
 {
     if (!p) return E_ARG;
@@ -472,18 +616,22 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
 {
     if (!p || (p->count && !d_sizes)) return E_ARG;
     if (reps < 1) reps = 1;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    struct Events {
+        cudaEvent_t e0, e1;
+        Events() { cudaEventCreate(&e0); cudaEventCreate(&e1); }
+        ~Events() { cudaEventDestroy(e0); cudaEventDestroy(e1); }
+    } ev;
+    cudaEvent_t e0 = ev.e0, e1 = ev.e1;
     float best = 1e30f;
-    int best_v = 0, best_c = 0;
+    int best_v = p->tma_ok ? 0 : 1, best_c = 0;
     for (int v = 0; v < kNumVariants; v++) {
+        if (kVariants[v].tma && !p->tma_ok) continue;
         int st = plan_layout(p, v, stream);
         if (st) return st;
         const void* fn = kVariants[v].kernel(p->type, p->dim, p->compress);
         int occ = 0;
-        const size_t smem = p->compress ? kVariants[v].smem(p->type, p->dim) : 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].warps * 32, smem);
+        const size_t smem = kVariants[v].smem(p->type, p->dim, p->compress);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].threads, smem);
         for (int c = 1; c <= std::max(1, occ); c++) {
             p->ctas_per_sm = c;
             plan_launch(p, d_sizes, stream);   // warm
@@ -501,8 +649,6 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
         }
         if (cuSZp_workspace_check(p->d_ws, p->ws_bytes, stream)) return E_TIMEOUT;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     int st = plan_layout(p, best_v, stream);
     p->ctas_per_sm = best_c;
     if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = E_CUDA;
@@ -512,6 +658,7 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
 extern "C" int cuSZp_batch_plan_set_config(cuszp_batch_plan_t p, int variant, int ctas_per_sm)
 {
     if (!p || variant < 0 || variant >= kNumVariants) return E_ARG;
+    if (kVariants[variant].tma && !p->tma_ok) return E_UNSUPPORTED;
     const int st = plan_layout(p, variant, 0);
     p->ctas_per_sm = ctas_per_sm;
     if (st) return st;
@@ -523,6 +670,7 @@ extern "C" void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t p, cudaStream_
     if (!p) return;
     if (p->d_items) cudaFreeAsync(p->d_items, stream);
     if (p->d_ws) cudaFreeAsync(p->d_ws, stream);
+    if (p->d_maps) cudaFreeAsync(p->d_maps, stream);
     delete p;
 }
 

@@ -159,7 +159,7 @@ static EncodeTiledFn encode_tiled()
 }
 
 // 2D/3D: the array as a 3D tensor (x fastest) with one data block per box.
-static bool make_block_map(CUtensorMap* m, const Problem& p, const void* in)
+bool make_block_map(CUtensorMap* m, const Problem& p, const void* in)
 {
     EncodeTiledFn enc = encode_tiled();
     if (!enc) return false;
@@ -211,8 +211,8 @@ static KernelRef tma_kernel_for(const Problem& p)
     return tma_pick<double, 3>(p.mode);
 }
 
-// CUSZP_NO_TMA=1 in the environment selects the cp.async compress kernels for every input.
-static bool tma_allowed()
+// CUSZP_NO_TMA=1 in the environment selects the cp.async kernels for every input.
+bool tma_allowed()
 {
     static const bool ok = [] {
         const char* e = std::getenv("CUSZP_NO_TMA");

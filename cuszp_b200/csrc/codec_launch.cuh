@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "codec.cuh"
@@ -46,6 +47,12 @@ size_t max_stream_bytes(const Problem& p);
 // (float for f32, double for f64 -- the generic API widens a float).
 int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double eb, void* ws, cudaStream_t s);
 int launch_decompress(const Problem& p, void* d_out, const uint8_t* d_cmp, double eb, void* ws, cudaStream_t s);
+
+// The TMA kernels: whether the environment allows them (CUSZP_NO_TMA=1 turns them
+// off), and the 2D/3D tensor map of an array (one data block per box; false when
+// the driver rejects the geometry, e.g. a row pitch that is not a multiple of 16 bytes).
+bool tma_allowed();
+bool make_block_map(CUtensorMap* m, const Problem& p, const void* data);
 
 // Value range (min, max) of a device array with the reference CLI's semantics
 // (examples/cuSZp.cpp:176-187): NaNs are skipped unless the first element is NaN.

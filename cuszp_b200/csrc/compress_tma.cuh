@@ -25,6 +25,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "codec_kernels.cuh"
 
 namespace cuszp {
@@ -154,8 +156,12 @@ struct TmaShared {
     uint64_t freed[C::NIN];            // input slot's rate pass done (one arrival per codec warp)
     uint64_t aggd[C::NC];              // tile aggregate posted (last codec warp)
     uint64_t based[C::NC];             // tile offset published (resolver)
-    int64_t tick[C::NIN];              // tile held by each input slot (>= ntiles: no more tiles)
+    int64_t tick[C::NIN];              // tile held by each input slot (>= total: no more tiles)
+    int64_t local[C::NIN];             // ... its index inside its array
     int64_t tile_of[C::NC];            // tile held by each code slot
+    int64_t local_of[C::NC];           // ... its index inside its array
+    int32_t arr[C::NIN];               // array of each input slot's tile (batches)
+    int32_t arr_of[C::NC];             // array of each code slot's tile
     unsigned long long agg[C::NC];     // tile payload bytes
     unsigned long long base[C::NC];    // tile payload offset (exclusive prefix)
     uint32_t wt[C::NC][C::WARPS];      // warp payload bytes
@@ -421,12 +427,49 @@ __device__ __forceinline__ void warp_copy_out(saddr_t src, uint32_t n, uint8_t* 
     }
 }
 
-// ------------------------------------------------------------------ the kernel
+// ------------------------------------------------------------------ tile sources
 
-template <typename T, int DIM, int MODE>
-__global__ void __launch_bounds__(TmaCfg<T, DIM>::THREADS, 2)
-compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ in, uint8_t* __restrict__ cmp,
-                    Geom g, T recip, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+// Where a tile's array lives: what the passes need beyond the tile's own data.
+struct TileArray {
+    void* data;                       // the array's elements (compress: read; decompress: written)
+    uint8_t* cmp;                     // its stream (compress: written; decompress: read)
+    const Geom* g;                    // its geometry
+    unsigned long long* status;       // its tile status words (indexed by local tile)
+    unsigned long long* total_out;    // its stream length
+    const CUtensorMap* tmap;          // its block boxes (2D/3D)
+    float eb;                         // its absolute bound (batches, where it is set on the device)
+    int mode;
+};
+
+// One array; everything is a kernel parameter and the encoding mode a constant.
+// `scale` is the reciprocal 0.5/eb when compressing and eb when decompressing.
+template <typename T, int MODE>
+struct SingleTiles {
+    const CUtensorMap* tmap;
+    void* data;
+    uint8_t* cmp;
+    const Geom* g;
+    T scale;
+    unsigned long long* status;
+    unsigned long long* total_out;
+    __device__ __forceinline__ uint64_t total() const { return g->ntiles; }
+    __device__ __forceinline__ void locate(int64_t t, int32_t& a, int64_t& local) const { a = 0; local = t; }
+    __device__ __forceinline__ TileArray array(int32_t) const
+    {
+        return TileArray{data, cmp, g, status, total_out, tmap, 0.f, MODE};
+    }
+    __device__ __forceinline__ T recip_of(const TileArray&) const { return scale; }
+    __device__ __forceinline__ T eb_of(const TileArray&) const { return scale; }
+    __device__ __forceinline__ void acquire_map(const CUtensorMap*) const {}   // a kernel parameter
+    template <typename F>
+    __device__ __forceinline__ void with_mode(int, F&& f) const { f(std::integral_constant<int, MODE>{}); }
+};
+
+// ------------------------------------------------------------------ the kernel body
+
+template <typename T, int DIM, typename Src>
+__device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __restrict__ hdr,
+                                                  unsigned long long* __restrict__ status_all)
 {
     using C = TmaCfg<T, DIM>;
     extern __shared__ unsigned char dsm[];
@@ -437,6 +480,7 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
     __shared__ __align__(8) TmaShared<T, DIM> sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t* err = &hdr->err;
+    const uint64_t ntotal = src.total();
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < C::NIN; i++) {
@@ -465,12 +509,13 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
                 if (*reinterpret_cast<volatile uint32_t*>(err)) break;
             }
             if (!ready) break;
-            const int64_t t = sh.tile_of[c];
+            const TileArray A = src.array(sh.arr_of[c]);
+            const int64_t lt = sh.local_of[c];
             const unsigned long long agg = sh.agg[c];
-            const uint64_t excl = t > 0 ? warp_lookback(status, t, err) : 0;
+            const uint64_t excl = lt > 0 ? warp_lookback(A.status, lt, err) : 0;
             if (lane == 0) {
-                if (t > 0) st_release(status + t, ST_INC | ((excl + agg) & ST_VAL));
-                if ((uint64_t)t == g.ntiles - 1) hdr->total = g.rate_bytes + excl + agg;
+                if (lt > 0) st_release(A.status + lt, ST_INC | ((excl + agg) & ST_VAL));
+                if ((uint64_t)lt == A.g->ntiles - 1) *A.total_out = A.g->rate_bytes + excl + agg;
                 sh.base[c] = excl;
                 mbar_arrive(&sh.based[c]);
             }
@@ -487,7 +532,7 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
             if (lane == 0) t = (int64_t)atomicAdd(&hdr->ticket, 1u);
             t = __shfl_sync(FULL, t, 0);
             T* dst = inbuf + s * C::TILE_ELEMS;
-            if ((uint64_t)t >= g.ntiles) {
+            if ((uint64_t)t >= ntotal) {
                 if (lane == 0) {
                     sh.tick[s] = t;
                     *reinterpret_cast<volatile int*>(&sh.kend) = issued - 1;   // issue order = tile order
@@ -495,8 +540,14 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
                 }
                 return false;
             }
+            int32_t a;
+            int64_t lt;
+            src.locate(t, a, lt);
+            const TileArray A = src.array(a);
+            const Geom g = *A.g;
+            const T* in = static_cast<const T*>(A.data);
             if constexpr (DIM == 1) {
-                const uint64_t e0 = (uint64_t)t * C::TILE_ELEMS;
+                const uint64_t e0 = (uint64_t)lt * C::TILE_ELEMS;
                 const uint64_t cnt = e0 < g.nbEle ? min((uint64_t)C::TILE_ELEMS, g.nbEle - e0) : 0;
                 const uint32_t bytes = (uint32_t)cnt * (uint32_t)sizeof(T);
                 const uint32_t main = bytes & ~15u;
@@ -505,23 +556,28 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
                 __syncwarp();
                 if (lane == 0) {
                     sh.tick[s] = t;
+                    sh.arr[s] = a;
+                    sh.local[s] = lt;
                     mbar_arrive_tx(&sh.full[s], main);
                     if (main) bulk_load(dst, in + e0, main, &sh.full[s]);
                 }
             } else {
-                const uint64_t b0 = (uint64_t)t * C::TB;
+                const uint64_t b0 = (uint64_t)lt * C::TB;
                 const uint32_t nvalid = (uint32_t)min((uint64_t)C::TB, g.nblocks - b0);
                 if (lane == 0) {
                     sh.tick[s] = t;
+                    sh.arr[s] = a;
+                    sh.local[s] = lt;
                     mbar_arrive_tx(&sh.full[s], nvalid * 64u * (uint32_t)sizeof(T));
                 }
                 __syncwarp();
+                if ((uint32_t)lane < nvalid) src.acquire_map(A.tmap);
                 for (uint32_t j = lane; j < nvalid; j += 32) {
                     const BlockPos p = block_pos(b0 + j, g);
                     if constexpr (DIM == 2)
-                        tma_load_3d(dst + j * 64, &tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, &sh.full[s]);
+                        tma_load_3d(dst + j * 64, A.tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, &sh.full[s]);
                     else
-                        tma_load_3d(dst + j * 64, &tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), &sh.full[s]);
+                        tma_load_3d(dst + j * 64, A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), &sh.full[s]);
                 }
             }
             return true;
@@ -531,7 +587,7 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
             const int s = k % C::NIN;
             __syncwarp();
             const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tick[s]);
-            if ((uint64_t)t >= g.ntiles) break;
+            if ((uint64_t)t >= ntotal) break;
             if (!mbar_wait(&sh.freed[s], (uint32_t)(k / C::NIN) & 1u, err)) break;
             if (!ended) ended = !issue(s);   // tile k's elements are consumed: load tile k + NIN
         }
@@ -550,10 +606,14 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
         auto pack_out = [&](int kk) -> bool {
             const int c = kk % C::NC;
             if (!mbar_wait(&sh.based[c], (uint32_t)(kk / C::NC) & 1u, err)) return false;
-            const uint32_t n =
-                pack_pass<DIM, MODE, C>(saddr(codebuf + c * C::TILE_ELEMS), saddr(sh.rates[c]), warp, region, lane);
+            const TileArray A = src.array(sh.arr_of[c]);
+            uint32_t n = 0;
+            src.with_mode(A.mode, [&](auto m) {
+                n = pack_pass<DIM, decltype(m)::value, C>(saddr(codebuf + c * C::TILE_ELEMS), saddr(sh.rates[c]), warp,
+                                                          region, lane);
+            });
             __syncwarp();
-            warp_copy_out(region, n, cmp + g.rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
+            warp_copy_out(region, n, A.cmp + A.g->rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
             __syncwarp();
             return true;
         };
@@ -562,14 +622,22 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
             const int s = k % C::NIN, c = k % C::NC;
             if (!mbar_wait(&sh.full[s], (uint32_t)(k / C::NIN) & 1u, err)) break;
             const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tick[s]);
-            if ((uint64_t)t >= g.ntiles) break;
+            if ((uint64_t)t >= ntotal) break;
+            const int32_t a = sh.arr[s];
+            const int64_t lt = sh.local[s];
+            const TileArray A = src.array(a);
+            const Geom g = *A.g;
+            const T recip = src.recip_of(A);
             const saddr_t tin = saddr(inbuf + s * C::TILE_ELEMS);
             const saddr_t code = saddr(codebuf + c * C::TILE_ELEMS);
-            uint32_t total;
-            if constexpr (DIM == 1)
-                total = rate_pass_1d<T, MODE>(tin, code, saddr(sh.rates[c]), warp, t, g, recip, cmp, lane);
-            else
-                total = rate_pass_nd<T, DIM, MODE>(tin, code, saddr(sh.rates[c]), warp, t, g, recip, cmp, lane);
+            uint32_t total = 0;
+            src.with_mode(A.mode, [&](auto m) {
+                constexpr int MODE = decltype(m)::value;
+                if constexpr (DIM == 1)
+                    total = rate_pass_1d<T, MODE>(tin, code, saddr(sh.rates[c]), warp, lt, g, recip, A.cmp, lane);
+                else
+                    total = rate_pass_nd<T, DIM, MODE>(tin, code, saddr(sh.rates[c]), warp, lt, g, recip, A.cmp, lane);
+            });
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&sh.freed[s]);   // this warp is done with the input slot
@@ -585,8 +653,10 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
                     }
                     sh.agg[c] = acc;
                     sh.tile_of[c] = t;
+                    sh.arr_of[c] = a;
+                    sh.local_of[c] = lt;
                     sh.cnt[c] = 0;
-                    st_release(status + t, (t == 0 ? ST_INC : ST_AGG) | acc);
+                    st_release(A.status + lt, (lt == 0 ? ST_INC : ST_AGG) | acc);
                     mbar_arrive(&sh.aggd[c]);
                 }
             }
@@ -595,7 +665,17 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
         for (int kk = k - C::DEFER < 0 ? 0 : k - C::DEFER; kk < k; kk++)
             if (!pack_out(kk)) break;
     }
-    finish_cta(hdr, status, g.ntiles);
+    finish_cta(hdr, status_all, ntotal);
+}
+
+template <typename T, int DIM, int MODE>
+__global__ void __launch_bounds__(TmaCfg<T, DIM>::THREADS, 2)
+compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ in, uint8_t* __restrict__ cmp,
+                    const __grid_constant__ Geom g, T recip, WsHeader* __restrict__ hdr,
+                    unsigned long long* __restrict__ status)
+{
+    const SingleTiles<T, MODE> src{&tmap, const_cast<T*>(in), cmp, &g, recip, status, &hdr->total};
+    compress_tma_body<T, DIM>(src, hdr, status);
 }
 
 }  // namespace cuszp

@@ -48,7 +48,9 @@ struct DecShared {
     using C = DecCfg<T, DIM>;
     uint64_t full[C::FRONT];           // slot filled (payload bytes + front arrival)
     uint64_t freed[C::FRONT];          // slot decoded (one arrival per codec warp)
-    int64_t tile[C::FRONT];            // tile in each slot (>= ntiles: the front warp has ended)
+    int64_t tile[C::FRONT];            // tile in each slot (>= total: the front warp has ended)
+    int64_t local[C::FRONT];           // ... its index inside its array
+    int32_t arr[C::FRONT];             // ... its array (batches)
     uint32_t poff[C::FRONT];           // payload start inside the slot
     uint32_t woff[C::FRONT][C::WARPS]; // codec warp offsets inside the tile payload
     uint8_t rates[C::FRONT][C::TB];    // block rate bytes
@@ -217,12 +219,105 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-// ------------------------------------------------------------------ the kernel
+// Decodes a codec warp's blocks of the tile in payload slot f into its output buffer
+// `ob` and starts their stores (the caller waits for the previous stores first).
+template <typename T, int DIM, int MODE, typename Src>
+__device__ __forceinline__ void decode_and_store(const Src& src, const TileArray& A, DecShared<T, DIM>& sh, int f,
+                                                 int64_t lt, saddr_t pay, T* ob, saddr_t obs, const XposeLane& xl,
+                                                 bool& stored, int warp, int lane)
+{
+    using C = DecCfg<T, DIM>;
+    const Geom g = *A.g;
+    const T eb = src.eb_of(A);
+    T* out = static_cast<T*>(A.data);
+    const bool bad = sh.poff[f] == kBadSlot;
+    // this warp's blocks: rate bytes, payload offsets (lane j: block j)
+    const uint32_t myr = lane < C::BPW && !bad ? sh.rates[f][warp * C::BPW + lane] : 0u;
+    const uint32_t mysz = lane < C::BPW ? payload_size<DIM, MODE>(myr) : 0u;
+    uint32_t incl = mysz;
+#pragma unroll
+    for (int o = 1; o < C::BPW; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][warp] + incl - mysz;
+    // the output buffer is free once the previous stores have read it
+    if (stored) bulk_wait_read();
+    __syncwarp();
+    const uint64_t b0 = (uint64_t)lt * C::TB + (uint64_t)warp * C::BPW;
+    if constexpr (DIM == 1) {
+#pragma unroll 1
+        for (int j = 0; j < C::BPW; j += 2) {
+            const uint32_t rA = __shfl_sync(FULL, myr, j), rB = __shfl_sync(FULL, myr, j + 1);
+            const uint32_t oA = __shfl_sync(FULL, myo, j), oB = __shfl_sync(FULL, myo, j + 1);
+            int32_t dA, dB;
+            decode_pair_1d<MODE>(pay, rA, rB, oA, oB, dA, dB, lane, xl);
+            if constexpr (MODE != MODE_FIXED) {
+                int32_t z = 0;
+                lorenzo_inverse<1>(dA, z, lane);
+                lorenzo_inverse<1>(dB, z, lane);
+            }
+            // blocks without payload decode to 0.0
+            sts_val(obs + j * 32 * sizeof(T), payload_size<1, MODE>(rA) ? dequant(dA, eb) : T(0));
+            sts_val(obs + (j + 1) * 32 * sizeof(T), payload_size<1, MODE>(rB) ? dequant(dB, eb) : T(0));
+        }
+    } else {
+#pragma unroll 1
+        for (int j = 0; j < C::BPW; j += 2) {
+            const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
+            const uint32_t rb = __shfl_sync(FULL, myr, j + 1), obo = __shfl_sync(FULL, myo, j + 1);
+            int32_t d0a, d1a, d0b, d1b;
+            decode_pair_nd<MODE>(pay, ra, rb, oa, obo, d0a, d1a, d0b, d1b, lane, xl);
+            if constexpr (MODE != MODE_FIXED) {
+                lorenzo_inverse<DIM>(d0a, d1a, lane);
+                lorenzo_inverse<DIM>(d0b, d1b, lane);
+            }
+            const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb) == 0;
+            const saddr_t oj = obs + j * 64 * sizeof(T);
+            sts_val(oj, za ? T(0) : dequant(d0a, eb));
+            sts_val(oj + 32 * sizeof(T), za ? T(0) : dequant(d1a, eb));
+            sts_val(oj + 64 * sizeof(T), zb ? T(0) : dequant(d0b, eb));
+            sts_val(oj + 96 * sizeof(T), zb ? T(0) : dequant(d1b, eb));
+        }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sh.freed[f]);   // done with the payload slot
+    fence_proxy_async_smem();                  // decoded values -> async proxy
+    __syncwarp();
+    if constexpr (DIM == 1) {
+        // the warp's 512 contiguous elements, clipped to the array
+        const uint64_t e0 = b0 * 32;
+        const uint64_t cnt = e0 < g.nbEle ? min((uint64_t)(C::BPW * 32), g.nbEle - e0) : 0;
+        const uint32_t bytes = (uint32_t)cnt * (uint32_t)sizeof(T);
+        const uint32_t main = bytes & ~15u;
+        const uint32_t tail = (bytes - main) / (uint32_t)sizeof(T);
+        if ((uint32_t)lane < tail) out[e0 + main / sizeof(T) + lane] = ob[main / sizeof(T) + lane];
+        if (lane == 0 && main) {
+            bulk_store(out + e0, ob, main);
+            bulk_commit();
+            stored = true;
+        }
+    } else {
+        // lane j stores block j (bulk groups are per thread: each storing lane
+        // commits and later waits for its own)
+        if ((uint64_t)lane < C::BPW && b0 + lane < g.nblocks) {
+            const BlockPos p = block_pos(b0 + lane, g);
+            src.acquire_map(A.tmap);
+            if constexpr (DIM == 2)
+                tma_store_3d(A.tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, ob + lane * 64);
+            else
+                tma_store_3d(A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob + lane * 64);
+            bulk_commit();
+            stored = true;
+        }
+    }
+}
 
-template <typename T, int DIM, int MODE>
-__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
-decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const uint8_t* __restrict__ cmp,
-                      Geom g, T eb, WsHeader* __restrict__ hdr, unsigned long long* __restrict__ status)
+// ------------------------------------------------------------------ the kernel body
+
+template <typename T, int DIM, typename Src>
+__device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __restrict__ hdr,
+                                                    unsigned long long* __restrict__ status_all)
 {
     using C = DecCfg<T, DIM>;
     extern __shared__ unsigned char dsm[];
@@ -232,7 +327,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
     __shared__ __align__(8) DecShared<T, DIM> sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t* err = &hdr->err;
-
+    const uint64_t ntotal = src.total();
     if (threadIdx.x == 0) {
         for (int i = 0; i < C::FRONT; i++) {
             mbar_init(&sh.full[i], 1);
@@ -251,15 +346,22 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
             int64_t t = 0;
             if (lane == 0) t = (int64_t)atomicAdd(&hdr->ticket, 1u);
             t = __shfl_sync(FULL, t, 0);
-            if ((uint64_t)t >= g.ntiles) {
+            if ((uint64_t)t >= ntotal) {
                 if (lane == 0) {
                     sh.tile[f] = t;
                     mbar_arrive(&sh.full[f]);
                 }
                 break;
             }
+            int32_t a;
+            int64_t lt;
+            src.locate(t, a, lt);
+            const TileArray A = src.array(a);
+            const Geom g = *A.g;
+            const uint8_t* cmp = A.cmp;
+            unsigned long long* status = A.status;
             // rate bytes -> block sizes -> codec warp offsets and the tile aggregate
-            const uint64_t b0 = (uint64_t)t * C::TB;
+            const uint64_t b0 = (uint64_t)lt * C::TB;
             constexpr int PER = C::TB / 32;   // rate bytes per lane (4 in 1D, 2 in 2D/3D)
             uint32_t sz[PER], rsum = 0;
 #pragma unroll
@@ -267,7 +369,7 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                 const uint64_t b = b0 + (uint64_t)lane * PER + i;   // lane holds consecutive blocks
                 const uint32_t r = b < g.nblocks ? __ldg(cmp + b) : 0u;
                 sh.rates[f][lane * PER + i] = (uint8_t)r;
-                sz[i] = payload_size<DIM, MODE>(r);
+                src.with_mode(A.mode, [&](auto md) { sz[i] = payload_size<DIM, decltype(md)::value>(r); });
                 rsum += sz[i];
             }
             uint32_t incl = rsum;
@@ -281,11 +383,11 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
             constexpr int LPW = C::BPW / PER;   // lanes per codec warp
             if (lane % LPW == 0) sh.woff[f][lane / LPW] = incl - rsum;
             __syncwarp();   // rates and offsets are written before lane 0 publishes the slot
-            if (lane == 0) st_release(status + t, (t == 0 ? ST_INC : ST_AGG) | agg);
-            const uint64_t excl = t > 0 ? warp_lookback(status, t, err) : 0;
+            if (lane == 0) st_release(status + lt, (lt == 0 ? ST_INC : ST_AGG) | agg);
+            const uint64_t excl = lt > 0 ? warp_lookback(status, lt, err) : 0;
             if (lane == 0) {
-                if (t > 0) st_release(status + t, ST_INC | ((excl + agg) & ST_VAL));
-                if ((uint64_t)t == g.ntiles - 1) hdr->total = g.rate_bytes + excl + agg;
+                if (lt > 0) st_release(status + lt, ST_INC | ((excl + agg) & ST_VAL));
+                if ((uint64_t)lt == g.ntiles - 1) *A.total_out = g.rate_bytes + excl + agg;
                 const uint64_t p0 = g.rate_bytes + excl, p1 = p0 + agg;
                 const uint64_t a0 = p0 & ~15ull, a1 = (p1 + 15) & ~15ull;
                 // rate bytes no valid stream holds (rate > 32 outside outlier mode) could
@@ -294,6 +396,8 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
                 if (!fits) atomicOr(err, ERR_CAPACITY);
                 const uint32_t bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
                 sh.tile[f] = t;
+                sh.local[f] = lt;
+                sh.arr[f] = a;
                 sh.poff[f] = fits ? (uint32_t)(p0 - a0) : kBadSlot;
                 mbar_arrive_tx(&sh.full[f], bytes);
                 if (bytes) bulk_load(slot, cmp + a0, bytes, &sh.full[f]);
@@ -315,94 +419,29 @@ decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ 
             parity ^= 1u << f;
             if (!mbar_wait(&sh.full[f], ph, err)) break;
             const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tile[f]);
-            if ((uint64_t)t >= g.ntiles) { ended |= 1u << f; continue; }
+            if ((uint64_t)t >= ntotal) { ended |= 1u << f; continue; }
+            const TileArray A = src.array(sh.arr[f]);
+            const int64_t lt = sh.local[f];
             const saddr_t pay = saddr(slots + f * C::SLOT);
-            const bool bad = sh.poff[f] == kBadSlot;
-            // this warp's blocks: rate bytes, payload offsets (lane j: block j)
-            const uint32_t myr = lane < C::BPW && !bad ? sh.rates[f][warp * C::BPW + lane] : 0u;
-            const uint32_t mysz = lane < C::BPW ? payload_size<DIM, MODE>(myr) : 0u;
-            uint32_t incl = mysz;
-#pragma unroll
-            for (int o = 1; o < C::BPW; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][warp] + incl - mysz;
-            // the output buffer is free once the previous stores have read it
-            if (stored) bulk_wait_read();
-            __syncwarp();
-            const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-            if constexpr (DIM == 1) {
-#pragma unroll 1
-                for (int j = 0; j < C::BPW; j += 2) {
-                    const uint32_t rA = __shfl_sync(FULL, myr, j), rB = __shfl_sync(FULL, myr, j + 1);
-                    const uint32_t oA = __shfl_sync(FULL, myo, j), oB = __shfl_sync(FULL, myo, j + 1);
-                    int32_t dA, dB;
-                    decode_pair_1d<MODE>(pay, rA, rB, oA, oB, dA, dB, lane, xl);
-                    if constexpr (MODE != MODE_FIXED) {
-                        int32_t z = 0;
-                        lorenzo_inverse<1>(dA, z, lane);
-                        lorenzo_inverse<1>(dB, z, lane);
-                    }
-                    // blocks without payload decode to 0.0
-                    sts_val(obs + j * 32 * sizeof(T), payload_size<1, MODE>(rA) ? dequant(dA, eb) : T(0));
-                    sts_val(obs + (j + 1) * 32 * sizeof(T), payload_size<1, MODE>(rB) ? dequant(dB, eb) : T(0));
-                }
-            } else {
-#pragma unroll 1
-                for (int j = 0; j < C::BPW; j += 2) {
-                    const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
-                    const uint32_t rb = __shfl_sync(FULL, myr, j + 1), obo = __shfl_sync(FULL, myo, j + 1);
-                    int32_t d0a, d1a, d0b, d1b;
-                    decode_pair_nd<MODE>(pay, ra, rb, oa, obo, d0a, d1a, d0b, d1b, lane, xl);
-                    if constexpr (MODE != MODE_FIXED) {
-                        lorenzo_inverse<DIM>(d0a, d1a, lane);
-                        lorenzo_inverse<DIM>(d0b, d1b, lane);
-                    }
-                    const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb) == 0;
-                    const saddr_t oj = obs + j * 64 * sizeof(T);
-                    sts_val(oj, za ? T(0) : dequant(d0a, eb));
-                    sts_val(oj + 32 * sizeof(T), za ? T(0) : dequant(d1a, eb));
-                    sts_val(oj + 64 * sizeof(T), zb ? T(0) : dequant(d0b, eb));
-                    sts_val(oj + 96 * sizeof(T), zb ? T(0) : dequant(d1b, eb));
-                }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&sh.freed[f]);   // done with the payload slot
-            fence_proxy_async_smem();                  // decoded values -> async proxy
-            __syncwarp();
-            if constexpr (DIM == 1) {
-                // the warp's 512 contiguous elements, clipped to the array
-                const uint64_t e0 = b0 * 32;
-                const uint64_t cnt = e0 < g.nbEle ? min((uint64_t)(C::BPW * 32), g.nbEle - e0) : 0;
-                const uint32_t bytes = (uint32_t)cnt * (uint32_t)sizeof(T);
-                const uint32_t main = bytes & ~15u;
-                const uint32_t tail = (bytes - main) / (uint32_t)sizeof(T);
-                if ((uint32_t)lane < tail) out[e0 + main / sizeof(T) + lane] = ob[main / sizeof(T) + lane];
-                if (lane == 0 && main) {
-                    bulk_store(out + e0, ob, main);
-                    bulk_commit();
-                    stored = true;
-                }
-            } else {
-                // lane j stores block j (bulk groups are per thread: each storing lane
-                // commits and later waits for its own)
-                if ((uint64_t)lane < C::BPW && b0 + lane < g.nblocks) {
-                    const BlockPos p = block_pos(b0 + lane, g);
-                    if constexpr (DIM == 2)
-                        tma_store_3d(&tmap, (int)(p.x * 8), (int)(p.y * 8), (int)p.z, ob + lane * 64);
-                    else
-                        tma_store_3d(&tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob + lane * 64);
-                    bulk_commit();
-                    stored = true;
-                }
-            }
+            src.with_mode(A.mode, [&](auto m) {
+                decode_and_store<T, DIM, decltype(m)::value>(src, A, sh, f, lt, pay, ob, obs, xl, stored, warp, lane);
+            });
             __syncwarp();
         }
         if (stored) bulk_wait_all();
         __syncwarp();
     }
-    finish_cta(hdr, status, g.ntiles);
+    finish_cta(hdr, status_all, ntotal);
+}
+
+template <typename T, int DIM, int MODE>
+__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
+decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const uint8_t* __restrict__ cmp,
+                      const __grid_constant__ Geom g, T eb, WsHeader* __restrict__ hdr,
+                      unsigned long long* __restrict__ status)
+{
+    const SingleTiles<T, MODE> src{&tmap, out, const_cast<uint8_t*>(cmp), &g, eb, status, &hdr->total};
+    decompress_tma_body<T, DIM>(src, hdr, status);
 }
 
 }  // namespace cuszp

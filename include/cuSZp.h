@@ -182,6 +182,10 @@ int cuSZp_batch_plan_execute(cuszp_batch_plan_t plan, unsigned long long* d_size
 int cuSZp_batch_plan_tune(cuszp_batch_plan_t plan, unsigned long long* d_sizes, int reps, cudaStream_t stream);
 int cuSZp_batch_plan_set_config(cuszp_batch_plan_t plan, int variant, int ctasPerSM);
 int cuSZp_batch_plan_config(cuszp_batch_plan_t plan, int* warps, int* blocksPerWarp, int* ctasPerSM);
+/* The kernel pair in use: variant index, threads per CTA, and whether it is the TMA
+ * pair (variant 0, chosen by default when every array and stream starts on a 16-byte
+ * boundary; set_config returns CUSZP_ERROR_UNSUPPORTED for it otherwise). */
+int cuSZp_batch_plan_variant(cuszp_batch_plan_t plan, int* variant, int* threadsPerBlock, int* tma);
 /* Absolute bounds the last execution used (derived on the device for rel items). */
 int cuSZp_batch_plan_eb(cuszp_batch_plan_t plan, float* errorBounds, cudaStream_t stream);
 /* Synchronize and report a timed-out device wait (CUSZP_ERROR_TIMEOUT). */
