@@ -283,9 +283,15 @@ __device__ __forceinline__ uint32_t payload_size(uint32_t rb)
 
 // ------------------------------------------------------------------ tile look-back
 
-__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v)
+// Posts a tile's status word (aggregate or inclusive prefix).  The word carries its
+// state and value together and publishes no other data, so the store needs no
+// release ordering: a relaxed store does not first wait for this thread's earlier
+// global writes (rate and payload bytes) to reach L2, which under load costs
+// microseconds on the look-back chain.  Should a tile's aggregate ever land after its
+// inclusive prefix, readers would only look further back; sums stay exact.
+__device__ __forceinline__ void st_post(unsigned long long* p, unsigned long long v)
 {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
 // Status words carry their value (state and prefix in one 64-bit word), so polling
 // needs no acquire ordering; relaxed loads let a lane's polls overlap instead of
@@ -426,10 +432,10 @@ __device__ __forceinline__ void scan_finish(int64_t tile, uint64_t ntiles, unsig
         const uint64_t agg = __shfl_sync(FULL, incl, WARPS - 1);
         __syncwarp();
         if (lane < WARPS) s_warp[lane] = incl - v;
-        if (lane == 0) st_release(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
+        if (lane == 0) st_post(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
         const uint64_t excl = tile > 0 ? warp_lookback(status, tile, err) : 0;
         if (lane == 0) {
-            if (tile > 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
+            if (tile > 0) st_post(status + tile, ST_INC | ((excl + agg) & ST_VAL));
             *s_base = excl;
             if ((uint64_t)tile == ntiles - 1) *total_out = rate_bytes + excl + agg;
         }

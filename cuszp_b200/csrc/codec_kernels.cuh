@@ -636,7 +636,7 @@ __device__ __forceinline__ void resolve_prev(const TileCtx& c, unsigned long lon
     if ((threadIdx.x >> 5) == 0) {
         const uint64_t excl = c.local > 0 ? warp_lookback(c.status, c.local, err) : 0;
         if (threadIdx.x == 0) {
-            if (c.local > 0) st_release(c.status + c.local, ST_INC | ((excl + agg) & ST_VAL));
+            if (c.local > 0) st_post(c.status + c.local, ST_INC | ((excl + agg) & ST_VAL));
             if ((uint64_t)c.local == c.g.ntiles - 1) *c.total_out = c.g.rate_bytes + excl + agg;
             sp.base = excl;
         }
@@ -663,7 +663,7 @@ __device__ __forceinline__ unsigned long long encode_tile(const T* __restrict__ 
         woff += w < warp ? t : 0u;
         agg += t;
     }
-    if (threadIdx.x == 0) st_release(c.status + c.local, (c.local == 0 ? ST_INC : ST_AGG) | agg);
+    if (threadIdx.x == 0) st_post(c.status + c.local, (c.local == 0 ? ST_INC : ST_AGG) | agg);
     compress_pack<T, DIM, MODE, Tl>(K, sb + woff);
     return agg;
 }
@@ -986,7 +986,7 @@ __device__ __forceinline__ void post_aggregate(uint32_t warp_total, int64_t tile
         __syncwarp();
         if (lane < WARPS) s_w[lane] = incl - v;
         if (lane == 0) {
-            st_release(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
+            st_post(status + tile, (tile == 0 ? ST_INC : ST_AGG) | agg);
             *s_agg = agg;
         }
     }
@@ -1004,7 +1004,7 @@ __device__ __forceinline__ uint64_t resolve_tile(int64_t tile, uint64_t ntiles, 
     if ((threadIdx.x >> 5) == 0) {
         const uint64_t excl = tile > 0 ? warp_lookback(status, tile, err) : 0;
         if (threadIdx.x == 0) {
-            if (tile > 0) st_release(status + tile, ST_INC | ((excl + agg) & ST_VAL));
+            if (tile > 0) st_post(status + tile, ST_INC | ((excl + agg) & ST_VAL));
             if ((uint64_t)tile == ntiles - 1) *total_out = rate_bytes + excl + agg;
             lb.excl = excl;
         }

@@ -514,7 +514,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
             const unsigned long long agg = sh.agg[c];
             const uint64_t excl = lt > 0 ? warp_lookback(A.status, lt, err) : 0;
             if (lane == 0) {
-                if (lt > 0) st_release(A.status + lt, ST_INC | ((excl + agg) & ST_VAL));
+                if (lt > 0) st_post(A.status + lt, ST_INC | ((excl + agg) & ST_VAL));
                 if ((uint64_t)lt == A.g->ntiles - 1) *A.total_out = A.g->rate_bytes + excl + agg;
                 sh.base[c] = excl;
                 mbar_arrive(&sh.based[c]);
@@ -656,7 +656,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                     sh.arr_of[c] = a;
                     sh.local_of[c] = lt;
                     sh.cnt[c] = 0;
-                    st_release(A.status + lt, (lt == 0 ? ST_INC : ST_AGG) | acc);
+                    st_post(A.status + lt, (lt == 0 ? ST_INC : ST_AGG) | acc);
                     mbar_arrive(&sh.aggd[c]);
                 }
             }

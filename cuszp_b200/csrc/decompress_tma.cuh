@@ -383,10 +383,10 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
             constexpr int LPW = C::BPW / PER;   // lanes per codec warp
             if (lane % LPW == 0) sh.woff[f][lane / LPW] = incl - rsum;
             __syncwarp();   // rates and offsets are written before lane 0 publishes the slot
-            if (lane == 0) st_release(status + lt, (lt == 0 ? ST_INC : ST_AGG) | agg);
+            if (lane == 0) st_post(status + lt, (lt == 0 ? ST_INC : ST_AGG) | agg);
             const uint64_t excl = lt > 0 ? warp_lookback(status, lt, err) : 0;
             if (lane == 0) {
-                if (lt > 0) st_release(status + lt, ST_INC | ((excl + agg) & ST_VAL));
+                if (lt > 0) st_post(status + lt, ST_INC | ((excl + agg) & ST_VAL));
                 if ((uint64_t)lt == g.ntiles - 1) *A.total_out = g.rate_bytes + excl + agg;
                 const uint64_t p0 = g.rate_bytes + excl, p1 = p0 + agg;
                 const uint64_t a0 = p0 & ~15ull, a1 = (p1 + 15) & ~15ull;
