@@ -3,24 +3,24 @@
 //
 // One CTA = 8 codec warps + 1 loader warp + RESOLVERS resolver warps.  Tiles are the
 // same as the other compress kernels' (128 blocks in 1D, 64 in 2D/3D), so the
-// workspace and stream are identical.  A tile goes through two passes, DEFER tiles
-// apart, so that its size is known -- and posted for the other CTAs' look-backs --
-// as soon as its data lands, while the bytes follow once its offset is known:
+// workspace and stream are identical.  A tile's bytes are produced at once but
+// written DEFER tiles later, once its offset is known:
 //
 //   loader warp: takes tile tickets and loads each tile into an input slot with the
 //     Tensor Memory Accelerator -- one `cp.async.bulk` of the tile's contiguous
 //     elements in 1D, one `cp.async.bulk.tensor.3d` box per data block in 2D/3D (the
 //     box lands in the block's element order, OOB elements zero-filled) -- completing
-//     on an mbarrier.  It refills a slot as soon as the tile's rate pass is done.
-//   codec warps, rate pass (tile k): quantize + Lorenzo delta from the input slot,
-//     codes into a code slot, block rates -> rate bytes; the last warp to finish
-//     posts the tile aggregate.
+//     on an mbarrier.  It refills a slot as soon as the codec warps are done with it.
+//   codec warps (tile k): quantize + Lorenzo delta from the input slot, block rates
+//     -> rate bytes, and sign maps + bit-planes packed into a span of the warp's
+//     staging ring; the last warp to finish posts the tile aggregate.
 //   resolver warps: resolver r runs the decoupled look-back of the CTA's tiles
-//     k = r, r + NC, ... (those of code slot r) and publishes their offsets.
-//   codec warps, pack pass (tile k - DEFER): sign maps and bit-planes from the code
-//     slot into a warp staging region, written to the stream with 16-byte stores at
-//     the published offset.
-// Every wait is bounded; on timeout the error word records it and the kernel ends.
+//     k = r, r + NC, ... (those of tile state r) and publishes their offsets.
+//   codec warps, DEFER tiles later: the span is written to the stream with 16-byte
+//     stores at the published offset.
+// Codes never go through shared memory, so the input slots can be deep (three for
+// f32, two for f64) at two CTAs per SM.  Every wait is bounded; on timeout the error
+// word records it and the kernel ends.
 #pragma once
 
 #include <cuda.h>
@@ -34,10 +34,10 @@ namespace cuszp {
 template <typename T, int DIM>
 struct TmaCfg {
     static constexpr int WARPS = 8;                           // codec warps
-    static constexpr int DEFER = 2;                           // tiles between rate and pack pass
-    static constexpr int NC = DEFER + 1;                      // code slots (4096 int32 codes each)
-    // One resolver per code slot: resolver r takes the tiles of slot r in order, so it
-    // never waits on a phase of a slot barrier whose previous phase is still open
+    static constexpr int DEFER = 2;                           // tiles between packing and writing out
+    static constexpr int NC = DEFER + 1;                      // tile states (sizes, offsets, barriers)
+    // One resolver per tile state: resolver r takes the tiles of state r in order, so it
+    // never waits on a phase of a state barrier whose previous phase is still open
     // (mbarrier parity waits cannot tell a phase two ahead from one behind).
     static constexpr int RESOLVERS = NC;
     static constexpr int LOADER = WARPS;                      // warp index of the loader
@@ -47,13 +47,17 @@ struct TmaCfg {
     static constexpr int BLK = DIM == 1 ? 32 : 64;            // elements per data block
     static constexpr int TILE_ELEMS = TB * BLK;               // 4096
     static constexpr int TILE_BYTES = TILE_ELEMS * (int)sizeof(T);
-    static constexpr int NIN = sizeof(T) == 4 ? 2 : 1;        // input slots
+    static constexpr int NIN = sizeof(T) == 4 ? 3 : 2;        // input slots
     static constexpr int MAXBLK = DIM == 1 ? 4 + 4 + 4 * 32 : 4 + 8 + 8 * 32;   // worst block payload
-    static constexpr int REGION = (BPW * MAXBLK + 4 + 15) / 16 * 16;           // + slack for word reads
+    // one warp's share of a tile at worst
+    static constexpr int REGION = (BPW * MAXBLK + 15) / 16 * 16;
+    static_assert(2 * REGION <= (sizeof(T) == 4 ? DEFER + 1 : 2) * REGION, "a span alone always fits");
+    // staging ring per codec warp (a circular buffer of its packed, not yet written
+    // spans): room for DEFER + 1 worst-case spans in f32, two in f64
+    static constexpr int RING = (sizeof(T) == 4 ? DEFER + 1 : 2) * REGION;
     static constexpr int OFF_IN = 0;
-    static constexpr int OFF_CODE = NIN * TILE_BYTES;
-    static constexpr int OFF_STG = OFF_CODE + NC * TILE_ELEMS * 4;
-    static constexpr int BYTES = OFF_STG + WARPS * REGION;
+    static constexpr int OFF_STG = NIN * TILE_BYTES;
+    static constexpr int BYTES = OFF_STG + WARPS * RING + 16;   // + what a copy-out may read past a ring
     static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }   // + base alignment
     static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
 };
@@ -153,242 +157,174 @@ template <typename T, int DIM>
 struct TmaShared {
     using C = TmaCfg<T, DIM>;
     uint64_t full[C::NIN];             // input slot loaded (TMA bytes + loader arrival)
-    uint64_t freed[C::NIN];            // input slot's rate pass done (one arrival per codec warp)
+    uint64_t freed[C::NIN];            // input slot consumed (one arrival per codec warp)
     uint64_t aggd[C::NC];              // tile aggregate posted (last codec warp)
     uint64_t based[C::NC];             // tile offset published (resolver)
     int64_t tick[C::NIN];              // tile held by each input slot (>= total: no more tiles)
     int64_t local[C::NIN];             // ... its index inside its array
-    int64_t tile_of[C::NC];            // tile held by each code slot
+    int64_t tile_of[C::NC];            // tile held by each tile state
     int64_t local_of[C::NC];           // ... its index inside its array
     int32_t arr[C::NIN];               // array of each input slot's tile (batches)
-    int32_t arr_of[C::NC];             // array of each code slot's tile
+    int32_t arr_of[C::NC];             // array of each tile state's tile
     unsigned long long agg[C::NC];     // tile payload bytes
     unsigned long long base[C::NC];    // tile payload offset (exclusive prefix)
     uint32_t wt[C::NC][C::WARPS];      // warp payload bytes
     uint32_t woff[C::NC][C::WARPS];    // warp offsets inside the tile
-    uint32_t cnt[C::NC];               // codec warps done with the tile's rate pass
+    uint32_t cnt[C::NC];               // codec warps done with the tile
     int kend;                          // index in this CTA's sequence of the first missing tile
-    uint8_t rates[C::NC][C::TB];       // block rate bytes
 };
 
-// ------------------------------------------------------------------ rate pass
+// ------------------------------------------------------------------ codes and payloads
 
-// 1D: codes of the warp's 16 blocks of tile `t` (elements in `tin`) into `code`, their
-// rate bytes to the stream and to `rates`; returns the warp's payload bytes.
-template <typename T, int MODE>
-__device__ __forceinline__ uint32_t rate_pass_1d(saddr_t tin, saddr_t code, saddr_t rates, int warp, int64_t t,
-                                                 const Geom& g, T recip, uint8_t* __restrict__ cmp, int lane)
+// A codec warp's codes of one tile, kept in registers from the code phase to the
+// pack phase: lane l holds element l (1D: of each block; 2D/3D: elements l and l+32).
+template <int DIM, typename C>
+struct WarpCodes {
+    int32_t c0[C::BPW];
+    int32_t c1[DIM == 1 ? 1 : C::BPW];
+    uint32_t rb;   // lane j < BPW: rate byte of block j
+};
+
+// 1D code phase: the warp's 16 blocks of tile `t` (elements in `tin`) -> codes, rate
+// bytes (to the stream and to K.rb).  Returns the warp's payload bytes.
+template <typename T, int MODE, typename C>
+__device__ __forceinline__ uint32_t codes_1d(saddr_t tin, WarpCodes<1, C>& K, int warp, int64_t t, const Geom& g,
+                                             T recip, uint8_t* __restrict__ cmp, int lane)
 {
-    using C = TmaCfg<T, 1>;
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-    uint32_t off = 0, rb = 0;
-    if (b0 * 32 < g.nbEle) {
-        const saddr_t wb = tin + (warp * C::BPW * 32 + lane) * (uint32_t)sizeof(T);
-        const saddr_t wc = code + (warp * C::BPW * 32 + lane) * 4u;
-        const bool ragged = (b0 + C::BPW) * 32 > g.nbEle;
-        auto step = [&](int j, bool mask) {
-            const int32_t qA = quantize(lds_val<T>(wb + j * 32 * sizeof(T)), recip);
-            const int32_t qB = quantize(lds_val<T>(wb + (j + 1) * 32 * sizeof(T)), recip);
-            int32_t cA = qA, cB = qB;
-            if constexpr (MODE != MODE_FIXED) {
-                const int32_t uA = __shfl_up_sync(FULL, qA, 1), uB = __shfl_up_sync(FULL, qB, 1);
-                cA = wsub(qA, lane ? uA : 0);
-                cB = wsub(qB, lane ? uB : 0);
-            }
-            if (mask) {
-                const uint64_t i = (b0 + j) * 32 + lane;
-                cA = i < g.nbEle ? cA : 0;
-                cB = i + 32 < g.nbEle ? cB : 0;
-            }
-            sts_u32(wc + j * 128, (uint32_t)cA);
-            sts_u32(wc + (j + 1) * 128, (uint32_t)cB);
-            const uint32_t rA = block_rate<1, MODE>(uabs(cA), 0u, lane);
-            const uint32_t rB = block_rate<1, MODE>(uabs(cB), 0u, lane);
-            if (lane == j) rb = rA;
-            if (lane == j + 1) rb = rB;
-            off += payload_size<1, MODE>(rA) + payload_size<1, MODE>(rB);
-        };
-        if (ragged) {
-#pragma unroll 1
-            for (int j = 0; j < C::BPW; j += 2) step(j, true);
-        } else {
-#pragma unroll 4
-            for (int j = 0; j < C::BPW; j += 2) step(j, false);
+    uint32_t off = 0;
+    K.rb = 0;
+    const saddr_t wb = tin + (warp * C::BPW * 32 + lane) * (uint32_t)sizeof(T);
+    const bool ragged = (b0 + C::BPW) * 32 > g.nbEle;   // also: no element at all
+#pragma unroll
+    for (int j = 0; j < C::BPW; j += 2) {
+        const int32_t qA = quantize(lds_val<T>(wb + j * 32 * sizeof(T)), recip);
+        const int32_t qB = quantize(lds_val<T>(wb + (j + 1) * 32 * sizeof(T)), recip);
+        int32_t cA = qA, cB = qB;
+        if constexpr (MODE != MODE_FIXED) {
+            const int32_t uA = __shfl_up_sync(FULL, qA, 1), uB = __shfl_up_sync(FULL, qB, 1);
+            cA = wsub(qA, lane ? uA : 0);
+            cB = wsub(qB, lane ? uB : 0);
         }
+        if (ragged) {   // elements past the array: code 0 (stale slot contents)
+            const uint64_t i = (b0 + j) * 32 + lane;
+            cA = i < g.nbEle ? cA : 0;
+            cB = i + 32 < g.nbEle ? cB : 0;
+        }
+        K.c0[j] = cA;
+        K.c0[j + 1] = cB;
+        const uint32_t rA = block_rate<1, MODE>(uabs(cA), 0u, lane);
+        const uint32_t rB = block_rate<1, MODE>(uabs(cB), 0u, lane);
+        if (lane == j) K.rb = rA;
+        if (lane == j + 1) K.rb = rB;
+        off += payload_size<1, MODE>(rA) + payload_size<1, MODE>(rB);
     }
-    if (lane < C::BPW) {
-        sts_u8(rates + warp * C::BPW + lane, rb);
-        if (b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)rb;
-    }
+    if (lane < C::BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)K.rb;
     return off;
 }
 
-// 2D/3D: same for the warp's 8 blocks (each block's 64 elements contiguous in `tin`),
-// two blocks per step so that their dependency chains overlap.
-template <typename T, int DIM, int MODE>
-__device__ __forceinline__ uint32_t rate_pass_nd(saddr_t tin, saddr_t code, saddr_t rates, int warp, int64_t t,
-                                                 const Geom& g, T recip, uint8_t* __restrict__ cmp, int lane)
+// 2D/3D code phase: the warp's 8 blocks (each block's 64 elements contiguous in `tin`).
+template <typename T, int DIM, int MODE, typename C>
+__device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, int warp, int64_t t, const Geom& g,
+                                             T recip, uint8_t* __restrict__ cmp, int lane)
 {
-    using C = TmaCfg<T, DIM>;
     constexpr uint32_t B = DIM == 2 ? 8 : 4;
-    static_assert(C::BPW % 2 == 0, "blocks are processed in pairs");
+    static_assert(C::BPW % 4 == 0, "blocks are coded four at a time");
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-    uint32_t off = 0, rbyte = 0;
-    if (b0 < g.nblocks) {
-        const saddr_t wb = tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);   // this lane's element
-        const saddr_t wc = code + (warp * C::BPW * 64 + lane) * 4u;
-        const BlockPos bp = block_pos(b0, g);
+    uint32_t off = 0;
+    K.rb = 0;
+    const saddr_t wb = tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);   // this lane's element
+    const uint32_t nblk = b0 < g.nblocks ? (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0) : 0u;
+    // partial blocks exist only along axes the block size does not divide
+    const bool ragged = (g.dx % B) || (g.dy % B) || (DIM == 3 && (g.dz % 4));
+    auto code_pair = [&](saddr_t blk, int32_t& c0, int32_t& c1) {
+        const int32_t q0 = quantize(lds_val<T>(blk), recip);
+        const int32_t q1 = quantize(lds_val<T>(blk + 32 * sizeof(T)), recip);
+        c0 = q0;
+        c1 = q1;
+        if constexpr (MODE != MODE_FIXED) {
+            int32_t p0, p1;
+            predecessors<DIM>(q0, q1, lane, p0, p1);
+            c0 = wsub(q0, p0);
+            c1 = wsub(q1, p1);
+        }
+    };
+    if (!ragged && nblk == C::BPW) {
+        // every block whole: no masks, four independent blocks per step
+#pragma unroll
+        for (int j = 0; j < C::BPW; j++) code_pair(wb + j * 64 * sizeof(T), K.c0[j], K.c1[j]);
+    } else {
+        // blocks past the warp's last (nblk) or elements past the array: code 0
+        const BlockPos bp = block_pos(b0 < g.nblocks ? b0 : 0, g);
         uint32_t bx = bp.x, by = bp.y, bz = bp.z;
-        // this lane's element coordinates inside a block (halves 0 and 1)
         const uint32_t cx = DIM == 2 ? (lane & 7) : (lane & 3);
         const uint32_t ry0 = DIM == 2 ? (lane >> 3) : ((lane >> 2) & 3);
         const uint32_t ry1 = DIM == 2 ? ry0 + 4 : ry0;
         const uint32_t rz0 = DIM == 2 ? 0 : (lane >> 4);
         const uint32_t rz1 = DIM == 2 ? 0 : rz0 + 2;
-        const uint32_t nblk = (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0);
-        // partial blocks exist only along axes the block size does not divide
-        const bool ragged = (g.dx % B) || (g.dy % B) || (DIM == 3 && (g.dz % 4));
-        auto advance = [&](uint32_t& x, uint32_t& y, uint32_t& z) {
-            if (++x == g.bxn) {
-                x = 0;
-                if (++y == g.byn) { y = 0; ++z; }
-            }
-        };
-        // codes of one block (elements outside the array: code 0)
-        auto codes = [&](saddr_t blk, uint32_t x, uint32_t y, uint32_t z, int32_t& c0, int32_t& c1) {
-            const int32_t q0 = quantize(lds_val<T>(blk), recip);
-            const int32_t q1 = quantize(lds_val<T>(blk + 32 * sizeof(T)), recip);
-            c0 = q0;
-            c1 = q1;
-            if constexpr (MODE != MODE_FIXED) {
-                int32_t p0, p1;
-                predecessors<DIM>(q0, q1, lane, p0, p1);
-                c0 = wsub(q0, p0);
-                c1 = wsub(q1, p1);
-            }
-            const uint32_t xb = x * B, yb = y * B, zb = DIM == 2 ? z : z * 4;
-            if (ragged && (xb + B > g.dx || yb + B > g.dy || (DIM == 3 && zb + 4 > g.dz))) {
-                const bool inx = xb + cx < g.dx;
-                const bool ok0 = inx && yb + ry0 < g.dy && (DIM == 2 || zb + rz0 < g.dz);
-                const bool ok1 = inx && yb + ry1 < g.dy && (DIM == 2 || zb + rz1 < g.dz);
-                c0 = ok0 ? c0 : 0;
-                c1 = ok1 ? c1 : 0;
-            }
-        };
-        if (!ragged && nblk == C::BPW) {
-            // every block whole: no masks, four independent blocks per step
 #pragma unroll
-            for (int j = 0; j < C::BPW; j += 4) {
-                int32_t c0[4], c1[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const saddr_t blk = wb + (j + u) * 64 * sizeof(T);
-                    const int32_t q0 = quantize(lds_val<T>(blk), recip);
-                    const int32_t q1 = quantize(lds_val<T>(blk + 32 * sizeof(T)), recip);
-                    c0[u] = q0;
-                    c1[u] = q1;
-                    if constexpr (MODE != MODE_FIXED) {
-                        int32_t p0, p1;
-                        predecessors<DIM>(q0, q1, lane, p0, p1);
-                        c0[u] = wsub(q0, p0);
-                        c1[u] = wsub(q1, p1);
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    sts_u32(wc + (j + u) * 256, (uint32_t)c0[u]);
-                    sts_u32(wc + (j + u) * 256 + 128, (uint32_t)c1[u]);
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const uint32_t r = block_rate<DIM, MODE>(uabs(c0[u]), uabs(c1[u]), lane);
-                    if (lane == j + u) rbyte = r;
-                    off += payload_size<DIM, MODE>(r);
-                }
+        for (int j = 0; j < C::BPW; j++) {
+            int32_t c0, c1;
+            code_pair(wb + j * 64 * sizeof(T), c0, c1);
+            const uint32_t xb = bx * B, yb = by * B, zb = DIM == 2 ? bz : bz * 4;
+            const bool inx = xb + cx < g.dx;
+            const bool ok0 = (uint32_t)j < nblk && inx && yb + ry0 < g.dy && (DIM == 2 || zb + rz0 < g.dz);
+            const bool ok1 = (uint32_t)j < nblk && inx && yb + ry1 < g.dy && (DIM == 2 || zb + rz1 < g.dz);
+            K.c0[j] = ok0 ? c0 : 0;
+            K.c1[j] = ok1 ? c1 : 0;
+            if (++bx == g.bxn) {
+                bx = 0;
+                if (++by == g.byn) { by = 0; ++bz; }
             }
-        } else {
-#pragma unroll 1
-        for (uint32_t j = 0; j < nblk; j += 2) {
-            uint32_t xb2 = bx, yb2 = by, zb2 = bz;
-            advance(xb2, yb2, zb2);
-            int32_t c0a, c1a, c0b, c1b;
-            codes(wb + j * 64 * sizeof(T), bx, by, bz, c0a, c1a);
-            codes(wb + (j + 1) * 64 * sizeof(T), xb2, yb2, zb2, c0b, c1b);   // inside the warp's 8 blocks
-            if (j + 1 >= nblk) { c0b = 0; c1b = 0; }             // past the last block: rate 0
-            const saddr_t ca = wc + j * 256;
-            sts_u32(ca, (uint32_t)c0a);
-            sts_u32(ca + 128, (uint32_t)c1a);
-            sts_u32(ca + 256, (uint32_t)c0b);
-            sts_u32(ca + 384, (uint32_t)c1b);
-            const uint32_t ra = block_rate<DIM, MODE>(uabs(c0a), uabs(c1a), lane);
-            const uint32_t rb = block_rate<DIM, MODE>(uabs(c0b), uabs(c1b), lane);
-            if (lane == (int)j) rbyte = ra;
-            if (lane == (int)j + 1) rbyte = rb;
-            off += payload_size<DIM, MODE>(ra) + payload_size<DIM, MODE>(rb);
-            bx = xb2; by = yb2; bz = zb2;
-            advance(bx, by, bz);
-        }
         }
     }
-    if (lane < C::BPW) {
-        sts_u8(rates + warp * C::BPW + lane, rbyte);
-        if (b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)rbyte;
+#pragma unroll
+    for (int j = 0; j < C::BPW; j++) {
+        const uint32_t r = block_rate<DIM, MODE>(uabs(K.c0[j]), uabs(K.c1[j]), lane);
+        if (lane == j) K.rb = r;
+        off += payload_size<DIM, MODE>(r);
     }
+    if (lane < C::BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)K.rb;
     return off;
 }
 
-// ------------------------------------------------------------------ pack pass
-
-// Sign maps and bit-planes of the warp's blocks (codes in `code`, rate bytes in
-// `rates`) into `region`; returns the payload bytes written there.
+// Pack phase: sign maps and bit-planes of the warp's blocks, in stream order at `out`.
 template <int DIM, int MODE, typename C>
-__device__ __forceinline__ uint32_t pack_pass(saddr_t code, saddr_t rates, int warp, saddr_t region, int lane)
+__device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t out, int lane, const XposeLane& xl)
 {
-    const saddr_t wc = code + (warp * C::BPW * C::BLK + lane) * 4u;   // this lane's code of block 0
-    const uint32_t mine = lane < C::BPW ? lds_u8(rates + warp * C::BPW + lane) : 0u;
-    const XposeLane xl(lane ^ 7);
+    const uint32_t mine = lane < C::BPW ? K.rb : 0u;
+    const uint32_t sz = lane < C::BPW ? payload_size<DIM, MODE>(mine) : 0u;
+    uint32_t incl = sz;
+#pragma unroll
+    for (int o = 1; o < C::BPW; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t myoff = incl - sz;
     if constexpr (DIM != 1) {
         const uint32_t n = MODE == MODE_OUTLIER ? (mine & 0x1fu) : mine;
         if (__all_sync(FULL, n <= 15)) {
-            // every block narrow: offsets up front, all pairs unrolled (no branches between)
-            const uint32_t sz = payload_size<DIM, MODE>(mine);
-            uint32_t incl = sz;
-#pragma unroll
-            for (int o = 1; o < C::BPW; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const uint32_t myoff = incl - sz;
+            // every block narrow: all pairs unrolled, no branches between them
 #pragma unroll
             for (int j = 0; j < C::BPW; j += 2) {
                 const uint32_t ra = __shfl_sync(FULL, mine, j), rb = __shfl_sync(FULL, mine, j + 1);
                 const uint32_t oa = __shfl_sync(FULL, myoff, j), ob = __shfl_sync(FULL, myoff, j + 1);
-                const saddr_t ca = wc + j * 256;
-                pack_pair_nd<MODE, true>(ra, rb, (int32_t)lds_u32(ca), (int32_t)lds_u32(ca + 128),
-                                         (int32_t)lds_u32(ca + 256), (int32_t)lds_u32(ca + 384), region + oa,
-                                         region + ob, lane, xl);
+                pack_pair_nd<MODE, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane,
+                                         xl);
             }
-            return __shfl_sync(FULL, incl, C::BPW - 1);
+            return;
         }
     }
-    uint32_t off = 0;
-#pragma unroll 1
+#pragma unroll
     for (int j = 0; j < C::BPW; j += 2) {
         const uint32_t ra = __shfl_sync(FULL, mine, j), rb = __shfl_sync(FULL, mine, j + 1);
-        const uint32_t sa = payload_size<DIM, MODE>(ra);
-        if (ra | rb) {
-            if constexpr (DIM == 1) {
-                pack_pair_1d<MODE>(ra, rb, (int32_t)lds_u32(wc + j * 128), (int32_t)lds_u32(wc + (j + 1) * 128),
-                                   region + off, region + off + sa, lane, xl);
-            } else {
-                const saddr_t ca = wc + j * 256;
-                pack_pair_nd<MODE>(ra, rb, (int32_t)lds_u32(ca), (int32_t)lds_u32(ca + 128), (int32_t)lds_u32(ca + 256),
-                                   (int32_t)lds_u32(ca + 384), region + off, region + off + sa, lane, xl);
-            }
-        }
-        off += sa + payload_size<DIM, MODE>(rb);
+        if ((ra | rb) == 0) continue;
+        const uint32_t oa = __shfl_sync(FULL, myoff, j), ob = __shfl_sync(FULL, myoff, j + 1);
+        if constexpr (DIM == 1)
+            pack_pair_1d<MODE>(ra, rb, K.c0[j], K.c0[j + 1], out + oa, out + ob, lane, xl);
+        else
+            pack_pair_nd<MODE>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane, xl);
     }
-    return off;
 }
 
 // Warp-cooperative write of `n` staged bytes (`src` 16-byte aligned in shared memory)
@@ -475,7 +411,6 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
     extern __shared__ unsigned char dsm[];
     unsigned char* base = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
     T* inbuf = reinterpret_cast<T*>(base + C::OFF_IN);
-    int32_t* codebuf = reinterpret_cast<int32_t*>(base + C::OFF_CODE);
     uint8_t* stg = base + C::OFF_STG;
     __shared__ __align__(8) TmaShared<T, DIM> sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -602,25 +537,69 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
         __syncwarp();
     } else {
         // ---------------------------------------------------------------- codec warps
-        const saddr_t region = saddr(stg + warp * C::REGION);
-        auto pack_out = [&](int kk) -> bool {
-            const int c = kk % C::NC;
-            if (!mbar_wait(&sh.based[c], (uint32_t)(kk / C::NC) & 1u, err)) return false;
-            const TileArray A = src.array(sh.arr_of[c]);
-            uint32_t n = 0;
-            src.with_mode(A.mode, [&](auto m) {
-                n = pack_pass<DIM, decltype(m)::value, C>(saddr(codebuf + c * C::TILE_ELEMS), saddr(sh.rates[c]), warp,
-                                                          region, lane);
-            });
-            __syncwarp();
-            warp_copy_out(region, n, A.cmp + A.g->rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
-            __syncwarp();
-            return true;
+        // The warp's staging ring is a circular buffer of the spans it packed but has
+        // not yet written out (at most two between tiles, oldest first in q0, q1).  A
+        // tile's span (its exact size is known before packing) goes at the 16-byte
+        // aligned write position, or at the start of the ring when it does not fit
+        // before the end; when neither is free of live spans, the oldest span is
+        // written out first (waiting for its offset).  `lap` counts wraps of the write
+        // position, so "ahead of the oldest span" needs no full/empty flag.
+        struct Span {
+            int k;        // CTA tile index (< 0: none)
+            uint32_t at;  // ring offset
+            int lap;      // ... and its lap
+            uint32_t n;   // payload bytes
         };
-        int k = 0;
-        for (;; k++) {
+        const saddr_t ring = saddr(stg + warp * C::RING);
+        const XposeLane xl(lane ^ 7);
+        Span q0{-1, 0, 0, 0}, q1{-1, 0, 0, 0};
+        uint32_t head = 0;   // write position
+        int lap = 0;
+        bool ok = true;
+        auto pop = [&]() -> bool {   // write the oldest span out
+            const int c = q0.k % C::NC;
+            const bool done = mbar_wait(&sh.based[c], (uint32_t)(q0.k / C::NC) & 1u, err);
+            if (done) {
+                const TileArray A = src.array(sh.arr_of[c]);
+                warp_copy_out(ring + q0.at, q0.n, A.cmp + A.g->rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
+                __syncwarp();
+            }
+            q0 = q1;
+            q1.k = -1;
+            return done;
+        };
+        // ring offset (and lap) for a new span of n bytes
+        auto place = [&](uint32_t n, int& span_lap) -> uint32_t {
+            for (;;) {
+                if (q0.k < 0) {   // empty ring: start over
+                    head = n;
+                    lap = 0;
+                    span_lap = 0;
+                    return 0;
+                }
+                const uint32_t h = (head + 15u) & ~15u;
+                if (lap == q0.lap) {   // free: [h, RING) and [0, q0.at)
+                    if (h + n <= (uint32_t)C::RING) {
+                        head = h + n;
+                        span_lap = lap;
+                        return h;
+                    }
+                    if (n <= q0.at) {
+                        head = n;
+                        span_lap = ++lap;
+                        return 0;
+                    }
+                } else if (h + n <= q0.at) {   // free: [h, q0.at)
+                    head = h + n;
+                    span_lap = lap;
+                    return h;
+                }
+                if (!pop()) ok = false;   // a timed-out wait still frees the span
+            }
+        };
+        for (int k = 0;; k++) {
             const int s = k % C::NIN, c = k % C::NC;
-            if (!mbar_wait(&sh.full[s], (uint32_t)(k / C::NIN) & 1u, err)) break;
+            if (!mbar_wait(&sh.full[s], (uint32_t)(k / C::NIN) & 1u, err)) { ok = false; break; }
             const int64_t t = *reinterpret_cast<volatile int64_t*>(&sh.tick[s]);
             if ((uint64_t)t >= ntotal) break;
             const int32_t a = sh.arr[s];
@@ -629,41 +608,48 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
             const Geom g = *A.g;
             const T recip = src.recip_of(A);
             const saddr_t tin = saddr(inbuf + s * C::TILE_ELEMS);
-            const saddr_t code = saddr(codebuf + c * C::TILE_ELEMS);
-            uint32_t total = 0;
             src.with_mode(A.mode, [&](auto m) {
                 constexpr int MODE = decltype(m)::value;
+                WarpCodes<DIM, C> K;
+                uint32_t total;
                 if constexpr (DIM == 1)
-                    total = rate_pass_1d<T, MODE>(tin, code, saddr(sh.rates[c]), warp, lt, g, recip, A.cmp, lane);
+                    total = codes_1d<T, MODE, C>(tin, K, warp, lt, g, recip, A.cmp, lane);
                 else
-                    total = rate_pass_nd<T, DIM, MODE>(tin, code, saddr(sh.rates[c]), warp, lt, g, recip, A.cmp, lane);
-            });
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(&sh.freed[s]);   // this warp is done with the input slot
-                sh.wt[c][warp] = total;
-                __threadfence_block();
-                if (atomicAdd(&sh.cnt[c], 1u) == C::WARPS - 1) {   // last warp of the tile
+                    total = codes_nd<T, DIM, MODE, C>(tin, K, warp, lt, g, recip, A.cmp, lane);
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&sh.freed[s]);   // this warp is done with the input slot
+                    sh.wt[c][warp] = total;
                     __threadfence_block();
-                    uint32_t acc = 0;
-                    for (int w = 0; w < C::WARPS; w++) {
-                        const uint32_t x = *reinterpret_cast<volatile uint32_t*>(&sh.wt[c][w]);
-                        sh.woff[c][w] = acc;
-                        acc += x;
+                    if (atomicAdd(&sh.cnt[c], 1u) == C::WARPS - 1) {   // last warp of the tile
+                        __threadfence_block();
+                        uint32_t acc = 0;
+                        for (int w = 0; w < C::WARPS; w++) {
+                            const uint32_t x = *reinterpret_cast<volatile uint32_t*>(&sh.wt[c][w]);
+                            sh.woff[c][w] = acc;
+                            acc += x;
+                        }
+                        sh.agg[c] = acc;
+                        sh.tile_of[c] = t;
+                        sh.arr_of[c] = a;
+                        sh.local_of[c] = lt;
+                        sh.cnt[c] = 0;
+                        st_post(A.status + lt, (lt == 0 ? ST_INC : ST_AGG) | acc);
+                        mbar_arrive(&sh.aggd[c]);
                     }
-                    sh.agg[c] = acc;
-                    sh.tile_of[c] = t;
-                    sh.arr_of[c] = a;
-                    sh.local_of[c] = lt;
-                    sh.cnt[c] = 0;
-                    st_post(A.status + lt, (lt == 0 ? ST_INC : ST_AGG) | acc);
-                    mbar_arrive(&sh.aggd[c]);
                 }
-            }
-            if (k >= C::DEFER && !pack_out(k - C::DEFER)) break;
+                int span_lap = 0;
+                const uint32_t at = place(total, span_lap);
+                pack_codes<DIM, MODE, C>(K, ring + at, lane, xl);
+                __syncwarp();
+                if (q0.k >= 0 && q0.k <= k - C::DEFER && !pop()) ok = false;
+                const Span e{k, at, span_lap, total};
+                if (q0.k < 0) q0 = e;
+                else q1 = e;
+            });
+            if (!ok) break;
         }
-        for (int kk = k - C::DEFER < 0 ? 0 : k - C::DEFER; kk < k; kk++)
-            if (!pack_out(kk)) break;
+        while (ok && q0.k >= 0) ok = pop();
     }
     finish_cta(hdr, status_all, ntotal);
 }
