@@ -400,6 +400,7 @@ struct cuszp_batch_plan {
     int ctas_per_sm = 0;       // 0: occupancy limit
     bool tma_ok = false;       // every array suits the TMA kernels (variant 0)
     CUtensorMap* d_maps = nullptr;   // per-array tensor maps of the TMA kernels (2D/3D)
+    std::vector<uint8_t> grouped;    // per array: its map is a grouped 2D map
     int sms = 148;
     std::vector<cuszp_batch_item_t> host_items;
     std::vector<BatchItem> items;
@@ -430,6 +431,7 @@ static int plan_layout(cuszp_batch_plan* p, int variant, cudaStream_t s)
         it.in = h.d_in;
         it.out = h.d_out;
         it.g = g;
+        it.g.grouped = (size_t)a < p->grouped.size() ? p->grouped[a] : 0u;   // read by the TMA kernels only
         it.tile_start = tiles;
         it.mode = h.mode;
         it.eb = h.rel ? 0.0f : h.errorBound;
@@ -472,6 +474,7 @@ static int plan_maps(cuszp_batch_plan* p, cudaStream_t s)
 {
     p->tma_ok = tma_allowed();
     std::vector<CUtensorMap> maps(p->dim == 1 ? 0 : (size_t)p->count);
+    p->grouped.assign((size_t)p->count, 0);
     for (int a = 0; a < p->count && p->tma_ok; a++) {
         const cuszp_batch_item_t& h = p->host_items[a];
         if (h.nbEle == 0) continue;   // no tiles
@@ -483,7 +486,9 @@ static int plan_maps(cuszp_batch_plan* p, cudaStream_t s)
             continue;
         }
         std::memset(&maps[a], 0, sizeof(CUtensorMap));
-        if (!make_block_map(&maps[a], pr, p->compress ? h.d_in : h.d_out)) p->tma_ok = false;
+        bool grouped = false;
+        if (!make_block_map(&maps[a], pr, p->compress ? h.d_in : h.d_out, &grouped)) p->tma_ok = false;
+        p->grouped[a] = grouped ? 1 : 0;
     }
     if (!p->tma_ok || maps.empty()) return OK;
     if (cudaMallocAsync((void**)&p->d_maps, sizeof(CUtensorMap) * maps.size(), s) != cudaSuccess) return E_CUDA;

@@ -81,7 +81,12 @@ struct Geom {
     uint64_t ntiles;       // tiles handed out (1D: covers the whole rate region)
     FastDiv div_bx;        // division by bxn
     FastDiv div_plane;     // division by bxn * byn
+    uint32_t grouped;      // TMA kernels, 2D: the tensor map's box is kGroup whole blocks
 };
+
+// Blocks per tensor-map box of the TMA kernels' grouped 2D maps (one codec warp's share
+// of a tile in 2D/3D).
+constexpr uint32_t kGroup = 8;
 
 // ------------------------------------------------------------------ scalar helpers
 

@@ -158,12 +158,32 @@ static EncodeTiledFn encode_tiled()
     return fn;
 }
 
-// 2D/3D: the array as a 3D tensor (x fastest) with one data block per box.
-bool make_block_map(CUtensorMap* m, const Problem& p, const void* in)
+// 2D/3D tensor map of an array for the TMA kernels.  2D arrays whose blocks are all
+// whole and whose block rows hold whole groups get a grouped map: the array as the 5D
+// tensor (column in block, row in block, block column, block row, slice), so that one
+// box of kGroup whole blocks lands in shared memory in block order (k = 8r + c per
+// block); *grouped is set then.  Otherwise the array as a 3D tensor (x fastest) with
+// one data block per box, out-of-array elements zero-filled on loads and clipped on
+// stores.
+bool make_block_map(CUtensorMap* m, const Problem& p, const void* in, bool* grouped)
 {
     EncodeTiledFn enc = encode_tiled();
+    *grouped = false;
     if (!enc) return false;
     const cuuint64_t esz = p.type == 0 ? 4 : 8;
+    const CUtensorMapDataType dt = p.type == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if (p.dim == 2 && p.g.dx % 8 == 0 && p.g.dy % 8 == 0 && p.g.bxn % kGroup == 0) {
+        const cuuint64_t dims5[5] = {8, 8, p.g.bxn, p.g.byn, p.g.dz};
+        const cuuint64_t strides5[4] = {p.g.dx * esz, 8 * esz, 8ull * p.g.dx * esz, (cuuint64_t)p.g.dx * p.g.dy * esz};
+        const cuuint32_t box5[5] = {8, 8, kGroup, 1, 1};
+        const cuuint32_t estr5[5] = {1, 1, 1, 1, 1};
+        if (enc(m, dt, 5, const_cast<void*>(in), dims5, strides5, box5, estr5, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
+            *grouped = true;
+            return true;
+        }
+    }
     const cuuint64_t dims[3] = {p.g.dx, p.g.dy, p.g.dz};
     const cuuint64_t strides[2] = {p.g.dx * esz, (cuuint64_t)p.g.dx * p.g.dy * esz};
     const cuuint32_t box[3] = {p.dim == 2 ? 8u : 4u, p.dim == 2 ? 8u : 4u, p.dim == 2 ? 1u : 4u};
@@ -228,7 +248,8 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
     if (!tma_allowed() || (reinterpret_cast<uintptr_t>(in) & 15u)) return -1;
     alignas(64) CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
-    if (p.dim != 1 && !make_block_map(&map, p, in)) return -1;
+    bool grouped = false;
+    if (p.dim != 1 && !make_block_map(&map, p, in, &grouped)) return -1;
     const KernelRef k = tma_kernel_for(p);
     static std::mutex mu;
     static int sms[64] = {0};
@@ -254,6 +275,7 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
     Geom g = p.g;
+    g.grouped = grouped ? 1u : 0u;
     float rf = 0.5f / (float)eb;
     double rd = 0.5 / eb;
     const void* src = in;
@@ -308,7 +330,8 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     if (!tma_allowed() || ((reinterpret_cast<uintptr_t>(cmp) | reinterpret_cast<uintptr_t>(out)) & 15u)) return -1;
     alignas(64) CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
-    if (p.dim != 1 && !make_block_map(&map, p, out)) return -1;
+    bool grouped = false;
+    if (p.dim != 1 && !make_block_map(&map, p, out, &grouped)) return -1;
     const KernelRef k = dtma_kernel_for(p);
     static std::mutex mu;
     static int sms[64] = {0};
@@ -333,6 +356,7 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
     Geom g = p.g;
+    g.grouped = grouped ? 1u : 0u;
     float ebf = (float)eb;
     void* dst = out;
     const void* src = cmp;

@@ -49,10 +49,11 @@ int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double e
 int launch_decompress(const Problem& p, void* d_out, const uint8_t* d_cmp, double eb, void* ws, cudaStream_t s);
 
 // The TMA kernels: whether the environment allows them (CUSZP_NO_TMA=1 turns them
-// off), and the 2D/3D tensor map of an array (one data block per box; false when
-// the driver rejects the geometry, e.g. a row pitch that is not a multiple of 16 bytes).
+// off), and the 2D/3D tensor map of an array (false when the driver rejects the
+// geometry, e.g. a row pitch that is not a multiple of 16 bytes).  *grouped: the map
+// is a grouped 2D map (kGroup whole blocks per box), to be recorded in Geom::grouped.
 bool tma_allowed();
-bool make_block_map(CUtensorMap* m, const Problem& p, const void* data);
+bool make_block_map(CUtensorMap* m, const Problem& p, const void* data, bool* grouped);
 
 // Value range (min, max) of a device array with the reference CLI's semantics
 // (examples/cuSZp.cpp:176-187): NaNs are skipped unless the first element is NaN.

@@ -60,6 +60,7 @@ struct TmaCfg {
     static constexpr int BYTES = OFF_STG + WARPS * RING + 16;   // + what a copy-out may read past a ring
     static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }   // + base alignment
     static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
+    static_assert(DIM == 1 || TB % kGroup == 0, "tiles hold whole groups");
 };
 
 // ------------------------------------------------------------------ mbarrier / TMA
@@ -141,6 +142,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
         ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+// kGroup whole 2D blocks from a grouped map (dims: column in block, row in block, block
+// column, block row, slice) into shared memory in block order, completing on `bar`.
+__device__ __forceinline__ void tma_load_group(void* dst, const CUtensorMap* map, int bx, int by, int z, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(bx), "r"(by), "r"(z),
+          "r"(smem_u32(bar))
         : "memory");
 }
 // `bytes` (a multiple of 16) contiguous bytes from global `src` (16-byte aligned).
@@ -507,6 +518,14 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 }
                 __syncwarp();
                 if ((uint32_t)lane < nvalid) src.acquire_map(A.tmap);
+                if (DIM == 2 && g.grouped) {
+                    // kGroup whole blocks per box, landing in block order (nvalid is a
+                    // multiple of kGroup: rows hold whole groups)
+                    if ((uint32_t)lane * kGroup < nvalid) {
+                        const BlockPos p = block_pos(b0 + lane * kGroup, g);
+                        tma_load_group(dst + lane * kGroup * 64, A.tmap, (int)p.x, (int)p.y, (int)p.z, &sh.full[s]);
+                    }
+                } else
                 for (uint32_t j = lane; j < nvalid; j += 32) {
                     const BlockPos p = block_pos(b0 + j, g);
                     if constexpr (DIM == 2)

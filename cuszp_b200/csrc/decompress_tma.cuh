@@ -39,6 +39,7 @@ struct DecCfg {
     static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }
     static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
     static_assert(FRONT <= 8, "slot parities are kept in one byte");
+    static_assert(DIM == 1 || BPW == (int)kGroup, "a codec warp's 2D blocks are one grouped box");
 };
 
 constexpr uint32_t kBadSlot = 0xffffffffu;   // poff of a tile whose rate bytes are invalid
@@ -208,6 +209,13 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int 
                  ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
                  : "memory");
 }
+// kGroup whole 2D blocks (block order in shared `src`) to a grouped map's box.
+__device__ __forceinline__ void tma_store_group(const CUtensorMap* map, int bx, int by, int z, const void* src)
+{
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(bx), "r"(by), "r"(z), "r"(smem_u32(src))
+                 : "memory");
+}
 // `bytes` (a multiple of 16) from shared `src` to global `dst` (16-byte aligned).
 __device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes)
 {
@@ -300,7 +308,16 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
     } else {
         // lane j stores block j (bulk groups are per thread: each storing lane
         // commits and later waits for its own)
-        if ((uint64_t)lane < C::BPW && b0 + lane < g.nblocks) {
+        if (DIM == 2 && g.grouped) {
+            // the warp's kGroup blocks are one box (a whole group, or none past the array)
+            if (lane == 0 && b0 < g.nblocks) {
+                const BlockPos p = block_pos(b0, g);
+                src.acquire_map(A.tmap);
+                tma_store_group(A.tmap, (int)p.x, (int)p.y, (int)p.z, ob);
+                bulk_commit();
+                stored = true;
+            }
+        } else if ((uint64_t)lane < C::BPW && b0 + lane < g.nblocks) {
             const BlockPos p = block_pos(b0 + lane, g);
             src.acquire_map(A.tmap);
             if constexpr (DIM == 2)

@@ -111,7 +111,7 @@ def _nd_arrays(dim, dtype, seed):
     if dim == 1:
         shapes = [(1,), (4097,), (70_001,), (32,), (300_000,)]
     elif dim == 2:
-        shapes = [(3, 20, 36), (1, 129, 260), (2, 8, 8), (5, 17, 4)]
+        shapes = [(3, 20, 36), (1, 129, 260), (2, 8, 8), (5, 17, 4), (3, 40, 128)]
     else:
         shapes = [(9, 10, 12), (33, 17, 64), (4, 4, 4), (7, 5, 4)]
     return [(torch.randn(s, generator=g, device="cuda", dtype=torch.float64).cumsum(-1) * 0.01).to(dtype).contiguous()

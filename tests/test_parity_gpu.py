@@ -101,6 +101,10 @@ SHAPES = [
     (2, (12, 9, 1), None),
     (2, (516, 301, 5), None),
     (2, (1028, 1031, 1), None),
+    # whole 8x8 blocks and block rows of whole groups of 8: the TMA kernels' grouped map
+    (2, (128, 40, 3), None),
+    (2, (512, 520, 1), None),
+    (2, (64, 8, 7), None),
     (3, (4, 1, 1), None),
     (3, (68, 37, 29), None),
     (3, (256, 130, 66), None),
