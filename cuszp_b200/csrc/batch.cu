@@ -291,7 +291,7 @@ decompress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t*
 
 struct Variant {
     int warps, bpw1, bpwn;   // codec warps per CTA; data blocks per codec warp in 1D and in 2D/3D
-    int threads;             // threads per CTA
+    int (*threads)(int type, bool comp);   // threads per CTA
     bool tma;                // warp-specialised TMA kernels: arrays on 16-byte boundaries only
     const void* (*kernel)(int type, int dim, bool comp);
     size_t (*smem)(int type, int dim, bool comp);   // dynamic shared memory (set on first use)
@@ -360,6 +360,15 @@ static size_t tma_batch_smem(bool comp)
                 : enable_smem(tma_batch_kernel<T, DIM>(false), DecCfg<T, DIM>::smem_bytes(), set[1]);
 }
 
+template <int N>
+static int fixed_threads(int, bool) { return N; }
+
+static int tma_threads(int type, bool comp)
+{
+    if (!comp) return DecCfg<float, 1>::THREADS;
+    return type == 0 ? TmaCfg<float, 1>::THREADS : TmaCfg<double, 1>::THREADS;
+}
+
 static const void* tk(int type, int dim, bool comp)
 {
     if (type == 0) return dim == 1 ? tma_batch_kernel<float, 1>(comp) : dim == 2 ? tma_batch_kernel<float, 2>(comp) : tma_batch_kernel<float, 3>(comp);
@@ -375,15 +384,16 @@ static size_t tks(int type, int dim, bool comp)
 // Variant 0 is the TMA kernel pair (8 codec warps; the same tiles as variant 1);
 // then the cp.async kernels as (warps per CTA, blocks per warp in 1D, in 2D/3D).
 static const Variant kVariants[] = {
-    {8, 16, 8, TmaCfg<float, 1>::THREADS, true, tk, tks},
-    {8, 16, 8, 256, false, kv<8, 16, 8>, ks<8, 16, 8>},
-    {4, 16, 8, 128, false, kv<4, 16, 8>, ks<4, 16, 8>},
-    {8, 8, 4, 256, false, kv<8, 8, 4>, ks<8, 8, 4>},
-    {16, 8, 4, 512, false, kv<16, 8, 4>, ks<16, 8, 4>},
+    {8, 16, 8, tma_threads, true, tk, tks},
+    {8, 16, 8, fixed_threads<256>, false, kv<8, 16, 8>, ks<8, 16, 8>},
+    {4, 16, 8, fixed_threads<128>, false, kv<4, 16, 8>, ks<4, 16, 8>},
+    {8, 8, 4, fixed_threads<256>, false, kv<8, 8, 4>, ks<8, 8, 4>},
+    {16, 8, 4, fixed_threads<512>, false, kv<16, 8, 4>, ks<16, 8, 4>},
 };
-static_assert(TmaCfg<float, 1>::THREADS == TmaCfg<double, 3>::THREADS &&
-                  DecCfg<float, 1>::THREADS == TmaCfg<float, 1>::THREADS,
-              "one thread count for every TMA batch kernel");
+static_assert(TmaCfg<float, 1>::THREADS == TmaCfg<float, 3>::THREADS &&
+                  TmaCfg<double, 1>::THREADS == TmaCfg<double, 3>::THREADS &&
+                  DecCfg<float, 1>::THREADS == DecCfg<double, 3>::THREADS,
+              "TMA thread counts depend on the element type and direction only");
 static_assert(TmaCfg<float, 1>::TB == 8 * 16 && TmaCfg<float, 2>::TB == 8 * 8, "TMA tiles as in variant 1");
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -519,7 +529,8 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     const void* fn = v.kernel(p->type, p->dim, p->compress);
     const size_t smem = v.smem(p->type, p->dim, p->compress);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, v.threads, smem);
+    const int threads = v.threads(p->type, p->compress);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem);
     if (occ < 1) occ = 1;
     const int per_sm = p->ctas_per_sm > 0 ? std::min(p->ctas_per_sm, occ) : occ;
     const uint64_t want = (uint64_t)p->sms * per_sm;
@@ -533,7 +544,7 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     void* args_cp[] = {(void*)&items, (void*)&map, (void*)&total, (void*)&hdr, (void*)&status, (void*)&d_sizes};
     void* args_tma[] = {(void*)&items, (void*)&map, (void*)&maps, (void*)&total, (void*)&hdr, (void*)&status,
                         (void*)&d_sizes};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(v.threads), v.tma ? args_tma : args_cp, smem, s) == cudaSuccess
+    return cudaLaunchKernel(fn, dim3(grid), dim3(threads), v.tma ? args_tma : args_cp, smem, s) == cudaSuccess
                ? OK
                : E_CUDA;
 }
@@ -601,7 +612,7 @@ extern "C" int cuSZp_batch_plan_variant(cuszp_batch_plan_t p, int* variant, int*
 {
     if (!p) return E_ARG;
     if (variant) *variant = p->variant;
-    if (threadsPerBlock) *threadsPerBlock = kVariants[p->variant].threads;
+    if (threadsPerBlock) *threadsPerBlock = kVariants[p->variant].threads(p->type, p->compress);
     if (tma) *tma = kVariants[p->variant].tma ? 1 : 0;
     return OK;
 }
@@ -636,7 +647,7 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
         const void* fn = kVariants[v].kernel(p->type, p->dim, p->compress);
         int occ = 0;
         const size_t smem = kVariants[v].smem(p->type, p->dim, p->compress);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].threads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].threads(p->type, p->compress), smem);
         for (int c = 1; c <= std::max(1, occ); c++) {
             p->ctas_per_sm = c;
             plan_launch(p, d_sizes, stream);   // warm

@@ -62,7 +62,8 @@ size_t max_stream_bytes(const Problem& p)
 
 struct KernelRef {
     const void* fn;
-    size_t smem;   // dynamic shared memory (compress: prefetch + staging buffers)
+    size_t smem;       // dynamic shared memory (compress: prefetch + staging buffers)
+    unsigned threads;  // threads per CTA
 };
 
 template <typename T, int DIM, int MODE>
@@ -78,10 +79,10 @@ static KernelRef ckernel()
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         set[dev] = true;
     }
-    return {fn, bytes};
+    return {fn, bytes, kThreads};
 }
 template <typename T, int DIM, int MODE>
-static KernelRef dkernel() { return {(const void*)decompress_kernel<T, DIM, MODE>, 0}; }
+static KernelRef dkernel() { return {(const void*)decompress_kernel<T, DIM, MODE>, 0, kThreads}; }
 
 template <typename T, int DIM>
 static KernelRef pick(bool comp, int mode)
@@ -206,7 +207,7 @@ static KernelRef tma_kernel()
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         set[dev] = true;
     }
-    return {fn, bytes};
+    return {fn, bytes, TmaCfg<T, DIM>::THREADS};
 }
 
 template <typename T, int DIM>
@@ -263,9 +264,7 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
         if (sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
         int& c = occ_cache[dev][p.type][p.dim - 1][p.mode];
         if (c == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, p.type == 0 ? TmaCfg<float, 1>::THREADS
-                                                                                : TmaCfg<double, 1>::THREADS,
-                                                          k.smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, k.threads, k.smem);
             if (c < 1) c = 1;
         }
         occ = c;
@@ -282,8 +281,7 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
     void* dst = cmp;
     void* args[] = {(void*)&map, (void*)&src, (void*)&dst, (void*)&g, p.type == 0 ? (void*)&rf : (void*)&rd,
                     (void*)&hdr, (void*)&status};
-    const unsigned threads = TmaCfg<float, 1>::THREADS;
-    return cudaLaunchKernel(k.fn, dim3(grid), dim3(threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
+    return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
 }
 
 template <typename T, int DIM, int MODE>
@@ -298,7 +296,7 @@ static KernelRef dtma_kernel()
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         set[dev] = true;
     }
-    return {fn, bytes};
+    return {fn, bytes, DecCfg<T, DIM>::THREADS};
 }
 
 template <typename T, int DIM>
@@ -339,7 +337,7 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return -1;
-    const unsigned threads = DecCfg<float, 1>::THREADS;
+    const unsigned threads = k.threads;
     int occ = 0;
     {
         std::lock_guard<std::mutex> lk(mu);

@@ -34,12 +34,17 @@ namespace cuszp {
 template <typename T, int DIM>
 struct TmaCfg {
     static constexpr int WARPS = 8;                           // codec warps
-    static constexpr int DEFER = 2;                           // tiles between packing and writing out
+    // tiles between packing and writing out: a tile's offset must be resolved by then
+    // (the look-back takes about as long as two f32 tiles, or three f64 tiles: f64
+    // tiles are load-bound and shorter)
+    static constexpr int DEFER = sizeof(T) == 4 ? 2 : 3;
     static constexpr int NC = DEFER + 1;                      // tile states (sizes, offsets, barriers)
-    // One resolver per tile state: resolver r takes the tiles of state r in order, so it
-    // never waits on a phase of a state barrier whose previous phase is still open
-    // (mbarrier parity waits cannot tell a phase two ahead from one behind).
-    static constexpr int RESOLVERS = NC;
+    // Resolver r takes the tiles k = r, r + RESOLVERS, ...; RESOLVERS divides NC, so each
+    // tile state has one resolver that takes its tiles in order and never waits on a
+    // phase of a state barrier whose previous phase is still open (mbarrier parity
+    // waits cannot tell a phase two ahead from one behind).
+    static constexpr int RESOLVERS = sizeof(T) == 4 ? 3 : 2;
+    static_assert(NC % RESOLVERS == 0, "each tile state has one resolver");
     static constexpr int LOADER = WARPS;                      // warp index of the loader
     static constexpr int THREADS = 32 * (WARPS + 1 + RESOLVERS);
     static constexpr int BPW = DIM == 1 ? 16 : 8;             // data blocks per codec warp
@@ -51,10 +56,10 @@ struct TmaCfg {
     static constexpr int MAXBLK = DIM == 1 ? 4 + 4 + 4 * 32 : 4 + 8 + 8 * 32;   // worst block payload
     // one warp's share of a tile at worst
     static constexpr int REGION = (BPW * MAXBLK + 15) / 16 * 16;
-    static_assert(2 * REGION <= (sizeof(T) == 4 ? DEFER + 1 : 2) * REGION, "a span alone always fits");
     // staging ring per codec warp (a circular buffer of its packed, not yet written
-    // spans): room for DEFER + 1 worst-case spans in f32, two in f64
-    static constexpr int RING = (sizeof(T) == 4 ? DEFER + 1 : 2) * REGION;
+    // spans): room for three worst-case spans in f32, two in f64 (typical spans are far
+    // smaller; one worst-case span is the least the allocator needs)
+    static constexpr int RING = (sizeof(T) == 4 ? 3 : 2) * REGION;
     static constexpr int OFF_IN = 0;
     static constexpr int OFF_STG = NIN * TILE_BYTES;
     static constexpr int BYTES = OFF_STG + WARPS * RING + 16;   // + what a copy-out may read past a ring
@@ -557,7 +562,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
     } else {
         // ---------------------------------------------------------------- codec warps
         // The warp's staging ring is a circular buffer of the spans it packed but has
-        // not yet written out (at most two between tiles, oldest first in q0, q1).  A
+        // not yet written out (at most DEFER between tiles, oldest first in q[0..]).  A
         // tile's span (its exact size is known before packing) goes at the 16-byte
         // aligned write position, or at the start of the ring when it does not fit
         // before the end; when neither is free of live spans, the oldest span is
@@ -571,7 +576,10 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
         };
         const saddr_t ring = saddr(stg + warp * C::RING);
         const XposeLane xl(lane ^ 7);
-        Span q0{-1, 0, 0, 0}, q1{-1, 0, 0, 0};
+        Span q[C::DEFER];   // live spans, oldest first; q[i].k < 0: none (then none after it)
+#pragma unroll
+        for (int i = 0; i < C::DEFER; i++) q[i] = Span{-1, 0, 0, 0};
+        Span& q0 = q[0];
         uint32_t head = 0;   // write position
         int lap = 0;
         bool ok = true;
@@ -583,8 +591,9 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 warp_copy_out(ring + q0.at, q0.n, A.cmp + A.g->rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
                 __syncwarp();
             }
-            q0 = q1;
-            q1.k = -1;
+#pragma unroll
+            for (int i = 0; i + 1 < C::DEFER; i++) q[i] = q[i + 1];
+            q[C::DEFER - 1].k = -1;
             return done;
         };
         // ring offset (and lap) for a new span of n bytes
@@ -663,8 +672,13 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 __syncwarp();
                 if (q0.k >= 0 && q0.k <= k - C::DEFER && !pop()) ok = false;
                 const Span e{k, at, span_lap, total};
-                if (q0.k < 0) q0 = e;
-                else q1 = e;
+                bool put = false;   // into the first free entry (compile-time indices only)
+#pragma unroll
+                for (int i = 0; i < C::DEFER; i++)
+                    if (!put && q[i].k < 0) {
+                        q[i] = e;
+                        put = true;
+                    }
             });
             if (!ok) break;
         }
