@@ -331,10 +331,10 @@ struct LookbackShared {
     unsigned long long excl;
 };
 
+template <int K = kLookbackPerLane>
 __device__ __forceinline__ uint64_t warp_lookback(unsigned long long* status, int64_t tile, uint32_t* err)
 {
     const int lane = threadIdx.x & 31;
-    constexpr int K = kLookbackPerLane;
     constexpr long long NONE = -(1ll << 62);
     uint64_t excl = 0;
     int64_t hi = tile - 1;

@@ -53,8 +53,9 @@ struct DecShared {
     int64_t local[C::FRONT];           // ... its index inside its array
     int32_t arr[C::FRONT];             // ... its array (batches)
     uint32_t poff[C::FRONT];           // payload start inside the slot
-    uint32_t woff[C::FRONT][C::WARPS]; // codec warp offsets inside the tile payload
-    uint8_t rates[C::FRONT][C::TB];    // block rate bytes
+    // per slot and fill parity (the front warp prepares fill m while fill m - 1 decodes):
+    uint32_t woff[C::FRONT][2][C::WARPS];   // codec warp offsets inside the tile payload
+    uint8_t rates[C::FRONT][2][C::TB];      // block rate bytes
 };
 
 // ------------------------------------------------------------------ payload words
@@ -231,8 +232,8 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // `ob` and starts their stores (the caller waits for the previous stores first).
 template <typename T, int DIM, int MODE, typename Src>
 __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray& A, DecShared<T, DIM>& sh, int f,
-                                                 int64_t lt, saddr_t pay, T* ob, saddr_t obs, const XposeLane& xl,
-                                                 bool& stored, int warp, int lane)
+                                                 int rb, int64_t lt, saddr_t pay, T* ob, saddr_t obs,
+                                                 const XposeLane& xl, bool& stored, int warp, int lane)
 {
     using C = DecCfg<T, DIM>;
     const Geom g = *A.g;
@@ -240,7 +241,7 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
     T* out = static_cast<T*>(A.data);
     const bool bad = sh.poff[f] == kBadSlot;
     // this warp's blocks: rate bytes, payload offsets (lane j: block j)
-    const uint32_t myr = lane < C::BPW && !bad ? sh.rates[f][warp * C::BPW + lane] : 0u;
+    const uint32_t myr = lane < C::BPW && !bad ? sh.rates[f][rb][warp * C::BPW + lane] : 0u;
     const uint32_t mysz = lane < C::BPW ? payload_size<DIM, MODE>(myr) : 0u;
     uint32_t incl = mysz;
 #pragma unroll
@@ -248,7 +249,7 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
         const uint32_t v = __shfl_up_sync(FULL, incl, o);
         if (lane >= o) incl += v;
     }
-    const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][warp] + incl - mysz;
+    const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][rb][warp] + incl - mysz;
     // the output buffer is free once the previous stores have read it
     if (stored) bulk_wait_read();
     __syncwarp();
@@ -358,68 +359,77 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
         // ---------------------------------------------------------------- front warps
         const int f = warp - C::WARPS;
         uint8_t* slot = slots + f * C::SLOT;
+        // Fill m of the slot is prepared (ticket, rate bytes, aggregate, look-back)
+        // while the codec warps still decode fill m - 1; only the payload load waits
+        // for the slot.
         for (int m = 0;; m++) {
-            if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) break;
+            const int rb = m & 1;
             int64_t t = 0;
             if (lane == 0) t = (int64_t)atomicAdd(&hdr->ticket, 1u);
             t = __shfl_sync(FULL, t, 0);
-            if ((uint64_t)t >= ntotal) {
-                if (lane == 0) {
-                    sh.tile[f] = t;
-                    mbar_arrive(&sh.full[f]);
+            const bool end = (uint64_t)t >= ntotal;
+            int32_t a = 0;
+            int64_t lt = 0;
+            const uint8_t* cmp = nullptr;
+            uint64_t a0 = 0;
+            uint32_t bytes = 0, poff = 0;
+            if (!end) {
+                src.locate(t, a, lt);
+                const TileArray A = src.array(a);
+                const Geom g = *A.g;
+                cmp = A.cmp;
+                unsigned long long* status = A.status;
+                // rate bytes -> block sizes -> codec warp offsets and the tile aggregate
+                const uint64_t b0 = (uint64_t)lt * C::TB;
+                constexpr int PER = C::TB / 32;   // rate bytes per lane (4 in 1D, 2 in 2D/3D)
+                uint32_t sz[PER], rsum = 0;
+#pragma unroll
+                for (int i = 0; i < PER; i++) {
+                    const uint64_t b = b0 + (uint64_t)lane * PER + i;   // lane holds consecutive blocks
+                    const uint32_t r = b < g.nblocks ? __ldg(cmp + b) : 0u;
+                    sh.rates[f][rb][lane * PER + i] = (uint8_t)r;
+                    src.with_mode(A.mode, [&](auto md) { sz[i] = payload_size<DIM, decltype(md)::value>(r); });
+                    rsum += sz[i];
                 }
-                break;
-            }
-            int32_t a;
-            int64_t lt;
-            src.locate(t, a, lt);
-            const TileArray A = src.array(a);
-            const Geom g = *A.g;
-            const uint8_t* cmp = A.cmp;
-            unsigned long long* status = A.status;
-            // rate bytes -> block sizes -> codec warp offsets and the tile aggregate
-            const uint64_t b0 = (uint64_t)lt * C::TB;
-            constexpr int PER = C::TB / 32;   // rate bytes per lane (4 in 1D, 2 in 2D/3D)
-            uint32_t sz[PER], rsum = 0;
+                uint32_t incl = rsum;
 #pragma unroll
-            for (int i = 0; i < PER; i++) {
-                const uint64_t b = b0 + (uint64_t)lane * PER + i;   // lane holds consecutive blocks
-                const uint32_t r = b < g.nblocks ? __ldg(cmp + b) : 0u;
-                sh.rates[f][lane * PER + i] = (uint8_t)r;
-                src.with_mode(A.mode, [&](auto md) { sz[i] = payload_size<DIM, decltype(md)::value>(r); });
-                rsum += sz[i];
-            }
-            uint32_t incl = rsum;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const unsigned long long agg = __shfl_sync(FULL, incl, 31);
-            // codec warp w starts at block w * BPW = lane (w * BPW / PER)'s first block
-            constexpr int LPW = C::BPW / PER;   // lanes per codec warp
-            if (lane % LPW == 0) sh.woff[f][lane / LPW] = incl - rsum;
-            __syncwarp();   // rates and offsets are written before lane 0 publishes the slot
-            if (lane == 0) st_post(status + lt, (lt == 0 ? ST_INC : ST_AGG) | agg);
-            const uint64_t excl = lt > 0 ? warp_lookback(status, lt, err) : 0;
-            if (lane == 0) {
-                if (lt > 0) st_post(status + lt, ST_INC | ((excl + agg) & ST_VAL));
-                if ((uint64_t)lt == g.ntiles - 1) *A.total_out = g.rate_bytes + excl + agg;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const unsigned long long agg = __shfl_sync(FULL, incl, 31);
+                // codec warp w starts at block w * BPW = lane (w * BPW / PER)'s first block
+                constexpr int LPW = C::BPW / PER;   // lanes per codec warp
+                if (lane % LPW == 0) sh.woff[f][rb][lane / LPW] = incl - rsum;
+                if (lane == 0) st_post(status + lt, (lt == 0 ? ST_INC : ST_AGG) | agg);
+                const uint64_t excl = lt > 0 ? warp_lookback(status, lt, err) : 0;
+                if (lane == 0) {
+                    if (lt > 0) st_post(status + lt, ST_INC | ((excl + agg) & ST_VAL));
+                    if ((uint64_t)lt == g.ntiles - 1) *A.total_out = g.rate_bytes + excl + agg;
+                }
                 const uint64_t p0 = g.rate_bytes + excl, p1 = p0 + agg;
-                const uint64_t a0 = p0 & ~15ull, a1 = (p1 + 15) & ~15ull;
+                a0 = p0 & ~15ull;
+                const uint64_t a1 = (p1 + 15) & ~15ull;
                 // rate bytes no valid stream holds (rate > 32 outside outlier mode) could
                 // claim more than a slot: such a tile is not loaded and decodes to zeros
                 const bool fits = agg <= (unsigned long long)C::TB * C::MAXBLK;
-                if (!fits) atomicOr(err, ERR_CAPACITY);
-                const uint32_t bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
+                if (!fits && lane == 0) atomicOr(err, ERR_CAPACITY);
+                bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
+                poff = fits ? (uint32_t)(p0 - a0) : kBadSlot;
+            }
+            // the slot: fill m - 1 decoded
+            if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) break;
+            __syncwarp();   // rates and offsets are written before lane 0 publishes the fill
+            if (lane == 0) {
                 sh.tile[f] = t;
                 sh.local[f] = lt;
                 sh.arr[f] = a;
-                sh.poff[f] = fits ? (uint32_t)(p0 - a0) : kBadSlot;
+                sh.poff[f] = poff;
                 mbar_arrive_tx(&sh.full[f], bytes);
                 if (bytes) bulk_load(slot, cmp + a0, bytes, &sh.full[f]);
             }
             __syncwarp();
+            if (end) break;
         }
     } else {
         // ---------------------------------------------------------------- codec warps
@@ -441,7 +451,8 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
             const int64_t lt = sh.local[f];
             const saddr_t pay = saddr(slots + f * C::SLOT);
             src.with_mode(A.mode, [&](auto m) {
-                decode_and_store<T, DIM, decltype(m)::value>(src, A, sh, f, lt, pay, ob, obs, xl, stored, warp, lane);
+                decode_and_store<T, DIM, decltype(m)::value>(src, A, sh, f, (int)ph, lt, pay, ob, obs, xl, stored, warp,
+                                                             lane);
             });
             __syncwarp();
         }
