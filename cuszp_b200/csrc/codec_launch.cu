@@ -321,6 +321,18 @@ static KernelRef dtma_kernel_for(const Problem& p)
     return dtma_pick<double, 3>(p.mode);
 }
 
+// CUSZP_TICKET_TILES=1..4 in the environment fixes the TMA decompress kernel's tiles per
+// ticket (0: the size-based choice) -- for tests of both ticket forms on small arrays.
+static int ticket_tiles_override()
+{
+    static const int v = [] {
+        const char* e = std::getenv("CUSZP_TICKET_TILES");
+        const int x = e ? std::atoi(e) : 0;
+        return x >= 1 && x <= kMaxTicketTiles ? x : 0;
+    }();
+    return v;
+}
+
 // Decompress through the TMA kernel when the stream and the output start on 16-byte
 // boundaries; returns -1 when the caller should use the other decompress kernel.
 static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, void* ws, cudaStream_t s)
@@ -358,8 +370,13 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     float ebf = (float)eb;
     void* dst = out;
     const void* src = cmp;
+    // f64 tiles (32 KB of output) decode fast enough that the look-back chain limits:
+    // tickets of kMaxTicketTiles tiles when every front warp still gets two of them
+    const uint64_t front = (uint64_t)grid * DecCfg<double, 1>::FRONT;
+    int tickets = p.type == 1 && p.g.ntiles >= 2ull * kMaxTicketTiles * front ? kMaxTicketTiles : 1;
+    if (const int forced = ticket_tiles_override()) tickets = forced;
     void* args[] = {(void*)&map, (void*)&dst, (void*)&src, (void*)&g, p.type == 0 ? (void*)&ebf : (void*)&eb,
-                    (void*)&hdr, (void*)&status};
+                    (void*)&hdr, (void*)&status, (void*)&tickets};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
 }
 

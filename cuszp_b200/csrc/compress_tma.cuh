@@ -404,7 +404,9 @@ struct SingleTiles {
     T scale;
     unsigned long long* status;
     unsigned long long* total_out;
+    int tickets = 1;   // decompress: tiles per ticket (1 or up to kMaxTicketTiles)
     __device__ __forceinline__ uint64_t total() const { return g->ntiles; }
+    __device__ __forceinline__ int ticket_tiles() const { return tickets; }
     __device__ __forceinline__ void locate(int64_t t, int32_t& a, int64_t& local) const { a = 0; local = t; }
     __device__ __forceinline__ TileArray array(int32_t) const
     {
@@ -693,7 +695,7 @@ compress_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restric
                     const __grid_constant__ Geom g, T recip, WsHeader* __restrict__ hdr,
                     unsigned long long* __restrict__ status)
 {
-    const SingleTiles<T, MODE> src{&tmap, const_cast<T*>(in), cmp, &g, recip, status, &hdr->total};
+    const SingleTiles<T, MODE> src{&tmap, const_cast<T*>(in), cmp, &g, recip, status, &hdr->total, 1};
     compress_tma_body<T, DIM>(src, hdr, status);
 }
 

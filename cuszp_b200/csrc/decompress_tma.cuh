@@ -43,6 +43,7 @@ struct DecCfg {
 };
 
 constexpr uint32_t kBadSlot = 0xffffffffu;   // poff of a tile whose rate bytes are invalid
+constexpr int kMaxTicketTiles = 4;           // decompress: most tiles per ticket (one look-back each)
 
 template <typename T, int DIM>
 struct DecShared {
@@ -359,37 +360,54 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
         // ---------------------------------------------------------------- front warps
         const int f = warp - C::WARPS;
         uint8_t* slot = slots + f * C::SLOT;
-        // Fill m of the slot is prepared (ticket, rate bytes, aggregate, look-back)
-        // while the codec warps still decode fill m - 1; only the payload load waits
-        // for the slot.
-        for (int m = 0;; m++) {
-            const int rb = m & 1;
-            int64_t t = 0;
-            if (lane == 0) t = (int64_t)atomicAdd(&hdr->ticket, 1u);
-            t = __shfl_sync(FULL, t, 0);
-            const bool end = (uint64_t)t >= ntotal;
-            int32_t a = 0;
-            int64_t lt = 0;
-            const uint8_t* cmp = nullptr;
-            uint64_t a0 = 0;
-            uint32_t bytes = 0, poff = 0;
-            if (!end) {
-                src.locate(t, a, lt);
-                const TileArray A = src.array(a);
-                const Geom g = *A.g;
-                cmp = A.cmp;
-                unsigned long long* status = A.status;
-                // rate bytes -> block sizes -> codec warp offsets and the tile aggregate
-                const uint64_t b0 = (uint64_t)lt * C::TB;
-                constexpr int PER = C::TB / 32;   // rate bytes per lane (4 in 1D, 2 in 2D/3D)
-                uint32_t sz[PER], rsum = 0;
+        // A ticket is a group of G consecutive tiles of one array (G = Src::ticket_tiles(),
+        // up to kMaxTicketTiles for f64, 1 for f32): their rate bytes give every tile's
+        // payload size at once, and one status word per group carries the look-back, so
+        // the chain of inclusive prefixes advances G tiles per step.  The group's tiles
+        // then fill the slot one after another.  Fill m is prepared while the codec warps
+        // still decode fill m - 1; only its payload load waits for the slot.
+        constexpr int GM = sizeof(T) == 8 ? kMaxTicketTiles : 1;   // f32 tickets stay single tiles
+        constexpr int PER = C::TB / 32;   // rate bytes per lane and tile (4 in 1D, 2 in 2D/3D)
+        constexpr int LPW = C::BPW / PER; // lanes per codec warp
+        const int G = min(src.ticket_tiles(), GM);
+        int m = 0;                        // fills of the slot so far
+        for (;;) {
+            int64_t gi = 0;
+            if (lane == 0) gi = (int64_t)atomicAdd(&hdr->ticket, 1u);
+            gi = __shfl_sync(FULL, gi, 0);
+            const int64_t t0 = gi * G;
+            if ((uint64_t)t0 >= ntotal) {   // no more tiles: an empty fill ends the slot
+                if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) break;
+                if (lane == 0) {
+                    sh.tile[f] = t0;
+                    mbar_arrive(&sh.full[f]);
+                }
+                break;
+            }
+            const int n = (int)min((uint64_t)G, ntotal - (uint64_t)t0);   // tiles in the group
+            int32_t a;
+            int64_t lt0;
+            src.locate(t0, a, lt0);   // a group's tiles are consecutive tiles of one array
+            const TileArray A = src.array(a);
+            const Geom g = *A.g;
+            const uint8_t* cmp = A.cmp;
+            unsigned long long* status = A.status;
+            const int64_t grp = lt0 / G;   // status word of the group
+            // rate bytes -> block sizes -> per tile: warp offsets and aggregate
+            uint32_t rbyte[GM][PER], wo[GM], agg[GM];
+            unsigned long long gagg = 0;
 #pragma unroll
-                for (int i = 0; i < PER; i++) {
-                    const uint64_t b = b0 + (uint64_t)lane * PER + i;   // lane holds consecutive blocks
-                    const uint32_t r = b < g.nblocks ? __ldg(cmp + b) : 0u;
-                    sh.rates[f][rb][lane * PER + i] = (uint8_t)r;
-                    src.with_mode(A.mode, [&](auto md) { sz[i] = payload_size<DIM, decltype(md)::value>(r); });
-                    rsum += sz[i];
+            for (int i = 0; i < GM; i++) {
+                const uint64_t b0 = (uint64_t)(lt0 + i) * C::TB;
+                uint32_t rsum = 0;
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    const uint64_t b = b0 + (uint64_t)lane * PER + e;   // lane holds consecutive blocks
+                    const uint32_t r = i < n && b < g.nblocks ? __ldg(cmp + b) : 0u;
+                    rbyte[i][e] = r;
+                    uint32_t sz = 0;
+                    src.with_mode(A.mode, [&](auto md) { sz = payload_size<DIM, decltype(md)::value>(r); });
+                    rsum += sz;
                 }
                 uint32_t incl = rsum;
 #pragma unroll
@@ -397,39 +415,48 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
                     const uint32_t v = __shfl_up_sync(FULL, incl, o);
                     if (lane >= o) incl += v;
                 }
-                const unsigned long long agg = __shfl_sync(FULL, incl, 31);
-                // codec warp w starts at block w * BPW = lane (w * BPW / PER)'s first block
-                constexpr int LPW = C::BPW / PER;   // lanes per codec warp
-                if (lane % LPW == 0) sh.woff[f][rb][lane / LPW] = incl - rsum;
-                if (lane == 0) st_post(status + lt, (lt == 0 ? ST_INC : ST_AGG) | agg);
-                const uint64_t excl = lt > 0 ? warp_lookback(status, lt, err) : 0;
-                if (lane == 0) {
-                    if (lt > 0) st_post(status + lt, ST_INC | ((excl + agg) & ST_VAL));
-                    if ((uint64_t)lt == g.ntiles - 1) *A.total_out = g.rate_bytes + excl + agg;
-                }
-                const uint64_t p0 = g.rate_bytes + excl, p1 = p0 + agg;
-                a0 = p0 & ~15ull;
-                const uint64_t a1 = (p1 + 15) & ~15ull;
+                wo[i] = incl - rsum;
+                agg[i] = __shfl_sync(FULL, incl, 31);
+                gagg += agg[i];
+            }
+            if (lane == 0) st_post(status + grp, (grp == 0 ? ST_INC : ST_AGG) | gagg);
+            const uint64_t excl = grp > 0 ? warp_lookback(status, grp, err) : 0;
+            if (lane == 0) {
+                if (grp > 0) st_post(status + grp, ST_INC | ((excl + gagg) & ST_VAL));
+                if ((uint64_t)(lt0 + n) == g.ntiles) *A.total_out = g.rate_bytes + excl + gagg;
+            }
+            uint64_t p0 = g.rate_bytes + excl;   // payload start of the group's next tile
+            bool stop = false;
+#pragma unroll
+            for (int i = 0; i < GM; i++) {
+                if (i >= n) break;
+                const int rb = m & 1;
+#pragma unroll
+                for (int e = 0; e < PER; e++) sh.rates[f][rb][lane * PER + e] = (uint8_t)rbyte[i][e];
+                if (lane % LPW == 0) sh.woff[f][rb][lane / LPW] = wo[i];
+                const uint64_t p1 = p0 + agg[i];
+                const uint64_t a0 = p0 & ~15ull, a1 = (p1 + 15) & ~15ull;
                 // rate bytes no valid stream holds (rate > 32 outside outlier mode) could
                 // claim more than a slot: such a tile is not loaded and decodes to zeros
-                const bool fits = agg <= (unsigned long long)C::TB * C::MAXBLK;
+                const bool fits = agg[i] <= (uint32_t)(C::TB * C::MAXBLK);
                 if (!fits && lane == 0) atomicOr(err, ERR_CAPACITY);
-                bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
-                poff = fits ? (uint32_t)(p0 - a0) : kBadSlot;
+                const uint32_t bytes = agg[i] && fits ? (uint32_t)(a1 - a0) : 0u;
+                // the slot: fill m - 1 decoded
+                if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) { stop = true; break; }
+                __syncwarp();   // rates and offsets are written before lane 0 publishes the fill
+                if (lane == 0) {
+                    sh.tile[f] = t0 + i;
+                    sh.local[f] = lt0 + i;
+                    sh.arr[f] = a;
+                    sh.poff[f] = fits ? (uint32_t)(p0 - a0) : kBadSlot;
+                    mbar_arrive_tx(&sh.full[f], bytes);
+                    if (bytes) bulk_load(slot, cmp + a0, bytes, &sh.full[f]);
+                }
+                __syncwarp();
+                p0 = p1;
+                m++;
             }
-            // the slot: fill m - 1 decoded
-            if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) break;
-            __syncwarp();   // rates and offsets are written before lane 0 publishes the fill
-            if (lane == 0) {
-                sh.tile[f] = t;
-                sh.local[f] = lt;
-                sh.arr[f] = a;
-                sh.poff[f] = poff;
-                mbar_arrive_tx(&sh.full[f], bytes);
-                if (bytes) bulk_load(slot, cmp + a0, bytes, &sh.full[f]);
-            }
-            __syncwarp();
-            if (end) break;
+            if (stop) break;
         }
     } else {
         // ---------------------------------------------------------------- codec warps
@@ -466,9 +493,9 @@ template <typename T, int DIM, int MODE>
 __global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
 decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const uint8_t* __restrict__ cmp,
                       const __grid_constant__ Geom g, T eb, WsHeader* __restrict__ hdr,
-                      unsigned long long* __restrict__ status)
+                      unsigned long long* __restrict__ status, int ticket_tiles)
 {
-    const SingleTiles<T, MODE> src{&tmap, out, const_cast<uint8_t*>(cmp), &g, eb, status, &hdr->total};
+    const SingleTiles<T, MODE> src{&tmap, out, const_cast<uint8_t*>(cmp), &g, eb, status, &hdr->total, ticket_tiles};
     decompress_tma_body<T, DIM>(src, hdr, status);
 }
 
