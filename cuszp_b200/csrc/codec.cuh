@@ -319,12 +319,12 @@ __device__ __forceinline__ uint64_t warp_sum64(uint64_t v)
 // 32 x kLookbackPerLane predecessors per step (poll k reads the 32 consecutive
 // status words hi-32k-31 .. hi-32k, one per lane: coalesced).
 // The newest inclusive prefix in the window ends the walk; every tile newer than it
-// must have posted its aggregate.  With relaxed posts the newest inclusive prefix is
-// nearly always among the last 32 tiles, so one word per lane per poll is fastest
-// (measured: 3-9 % shorter kernels than 8 words per lane); older prefixes are
-// reached by further steps.  Only the polling warp spins (with exponential
-// back-off).  Every wait is bounded: on timeout the error bit is set and the partial
-// sum is returned, so no CTA can hang the GPU.
+// must have posted its aggregate; older prefixes are reached by further steps.  One
+// word per lane per poll measured fastest: 3-9 % shorter compress kernels than 8 words
+// per lane, and no decompress kernel gained from 4, 8 or 16 (each poll then costs more
+// loads and instructions than the steps it saves).  Only the polling warp spins (with
+// exponential back-off).  Every wait is bounded: on timeout the error bit is set and
+// the partial sum is returned, so no CTA can hang the GPU.
 constexpr int kLookbackPerLane = 1;
 
 struct LookbackShared {

@@ -456,7 +456,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
             const int c = k % C::NC;
             const uint32_t parity = (uint32_t)(k / C::NC) & 1u;
             bool ready = false;
-            for (int i = 0; i < 4 * kWaitLimit; i++) {   // tile k's rate pass done, or no tile k
+            for (int i = 0; i < 4 * kWaitLimit; i++) {   // tile k coded and its size posted, or no tile k
                 if (mbar_try_wait_ns(&sh.aggd[c], parity, kWaitSliceNs / 4)) { ready = true; break; }
                 if (k >= *reinterpret_cast<volatile int*>(&sh.kend)) break;
                 if (*reinterpret_cast<volatile uint32_t*>(err)) break;
