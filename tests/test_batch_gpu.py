@@ -77,7 +77,7 @@ def test_graph_replay_and_autotune_keep_bytes():
     torch.cuda.synchronize()
     first = [o[:s].clone() for o, s in zip(plan.outputs, plan.sizes.cpu().tolist())]
     cfg = plan.tune(reps=2)
-    assert cfg["threads_per_block"] in (128, 256, 384, 512)
+    assert cfg["threads_per_block"] % 32 == 0 and 0 < cfg["threads_per_block"] <= 1024
     assert cfg["tma"] == (cfg["variant"] == 0)
     plan.capture()
     for o in plan.outputs:
