@@ -293,7 +293,7 @@ decompress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t*
 
 struct Variant {
     int warps, bpw1, bpwn;   // codec warps per CTA; data blocks per codec warp in 1D and in 2D/3D
-    int (*threads)(int type, bool comp);   // threads per CTA
+    int (*threads)(int type, int dim, bool comp);   // threads per CTA
     bool tma;                // warp-specialised TMA kernels: arrays on 16-byte boundaries only
     const void* (*kernel)(int type, int dim, bool comp);
     size_t (*smem)(int type, int dim, bool comp);   // dynamic shared memory (set on first use)
@@ -363,11 +363,11 @@ static size_t tma_batch_smem(bool comp)
 }
 
 template <int N>
-static int fixed_threads(int, bool) { return N; }
+static int fixed_threads(int, int, bool) { return N; }
 
-static int tma_threads(int type, bool comp)
+static int tma_threads(int type, int dim, bool comp)
 {
-    if (!comp) return DecCfg<float, 1>::THREADS;
+    if (!comp) return dim == 1 ? DecCfg<float, 1>::THREADS : DecCfg<float, 2>::THREADS;
     return type == 0 ? TmaCfg<float, 1>::THREADS : TmaCfg<double, 1>::THREADS;
 }
 
@@ -394,8 +394,9 @@ static const Variant kVariants[] = {
 };
 static_assert(TmaCfg<float, 1>::THREADS == TmaCfg<float, 3>::THREADS &&
                   TmaCfg<double, 1>::THREADS == TmaCfg<double, 3>::THREADS &&
-                  DecCfg<float, 1>::THREADS == DecCfg<double, 3>::THREADS,
-              "TMA thread counts depend on the element type and direction only");
+                  DecCfg<float, 1>::THREADS == DecCfg<double, 1>::THREADS &&
+                  DecCfg<float, 2>::THREADS == DecCfg<double, 3>::THREADS,
+              "TMA thread counts: compress by element type, decompress by 1D or 2D/3D");
 static_assert(TmaCfg<float, 1>::TB == 8 * 16 && TmaCfg<float, 2>::TB == 8 * 8, "TMA tiles as in variant 1");
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -531,7 +532,7 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     const void* fn = v.kernel(p->type, p->dim, p->compress);
     const size_t smem = v.smem(p->type, p->dim, p->compress);
     int occ = 0;
-    const int threads = v.threads(p->type, p->compress);
+    const int threads = v.threads(p->type, p->dim, p->compress);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem);
     if (occ < 1) occ = 1;
     const int per_sm = p->ctas_per_sm > 0 ? std::min(p->ctas_per_sm, occ) : occ;
@@ -614,7 +615,7 @@ extern "C" int cuSZp_batch_plan_variant(cuszp_batch_plan_t p, int* variant, int*
 {
     if (!p) return E_ARG;
     if (variant) *variant = p->variant;
-    if (threadsPerBlock) *threadsPerBlock = kVariants[p->variant].threads(p->type, p->compress);
+    if (threadsPerBlock) *threadsPerBlock = kVariants[p->variant].threads(p->type, p->dim, p->compress);
     if (tma) *tma = kVariants[p->variant].tma ? 1 : 0;
     return OK;
 }
@@ -649,7 +650,8 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
         const void* fn = kVariants[v].kernel(p->type, p->dim, p->compress);
         int occ = 0;
         const size_t smem = kVariants[v].smem(p->type, p->dim, p->compress);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].threads(p->type, p->compress), smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].threads(p->type, p->dim, p->compress),
+                                                      smem);
         for (int c = 1; c <= std::max(1, occ); c++) {
             p->ctas_per_sm = c;
             plan_launch(p, d_sizes, stream);   // warm

@@ -372,7 +372,7 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     const void* src = cmp;
     // f64 tiles (32 KB of output) decode fast enough that the look-back chain limits:
     // tickets of kMaxTicketTiles tiles when every front warp still gets two of them
-    const uint64_t front = (uint64_t)grid * DecCfg<double, 1>::FRONT;
+    const uint64_t front = (uint64_t)grid * (k.threads / 32 - DecCfg<double, 1>::WARPS);   // front warps
     int tickets = p.type == 1 && p.g.ntiles >= 2ull * kMaxTicketTiles * front ? kMaxTicketTiles : 1;
     if (const int forced = ticket_tiles_override()) tickets = forced;
     void* args[] = {(void*)&map, (void*)&dst, (void*)&src, (void*)&g, p.type == 0 ? (void*)&ebf : (void*)&eb,
