@@ -286,7 +286,7 @@ decompress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t*
                             unsigned long long* __restrict__ status, unsigned long long* __restrict__ sizes)
 {
     const BatchTiles<T, false> src{items, tile_map, tmaps, total_tiles, status, sizes};
-    decompress_tma_body<T, DIM>(src, hdr, status);
+    decompress_tma_body<T, DIM, false>(src, hdr, status);
 }
 
 // ------------------------------------------------------------------ tile-shape variants

@@ -284,40 +284,41 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, s) == cudaSuccess ? OK : E_CUDA;
 }
 
-template <typename T, int DIM, int MODE>
+template <typename T, int DIM, int MODE, bool DIRECT = false>
 static KernelRef dtma_kernel()
 {
     static bool set[64] = {};   // the attribute is per device
-    const void* fn = (const void*)decompress_tma_kernel<T, DIM, MODE>;
-    constexpr size_t bytes = DecCfg<T, DIM>::smem_bytes();
+    const void* fn = (const void*)decompress_tma_kernel<T, DIM, MODE, DIRECT>;
+    constexpr size_t bytes = DecCfg<T, DIM, DIRECT>::smem_bytes();
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !set[dev]) {
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         set[dev] = true;
     }
-    return {fn, bytes, DecCfg<T, DIM>::THREADS};
+    return {fn, bytes, DecCfg<T, DIM, DIRECT>::THREADS};
 }
 
-template <typename T, int DIM>
+template <typename T, int DIM, bool DIRECT = false>
 static KernelRef dtma_pick(int mode)
 {
     switch (mode) {
-        case 0: return dtma_kernel<T, DIM, 0>();
-        case 1: return dtma_kernel<T, DIM, 1>();
-        default: return dtma_kernel<T, DIM, 2>();
+        case 0: return dtma_kernel<T, DIM, 0, DIRECT>();
+        case 1: return dtma_kernel<T, DIM, 1, DIRECT>();
+        default: return dtma_kernel<T, DIM, 2, DIRECT>();
     }
 }
 
-static KernelRef dtma_kernel_for(const Problem& p)
+// grouped: a grouped 2D map (the direct-store kernel)
+static KernelRef dtma_kernel_for(const Problem& p, bool grouped)
 {
     if (p.type == 0) {
         if (p.dim == 1) return dtma_pick<float, 1>(p.mode);
-        if (p.dim == 2) return dtma_pick<float, 2>(p.mode);
+        if (p.dim == 2) return grouped ? dtma_pick<float, 2, true>(p.mode) : dtma_pick<float, 2>(p.mode);
         return dtma_pick<float, 3>(p.mode);
     }
     if (p.dim == 1) return dtma_pick<double, 1>(p.mode);
-    if (p.dim == 2) return dtma_pick<double, 2>(p.mode);
+    if (p.dim == 2) return grouped ? dtma_pick<double, 2, true>(p.mode) : dtma_pick<double, 2>(p.mode);
     return dtma_pick<double, 3>(p.mode);
 }
 
@@ -342,10 +343,10 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     std::memset(&map, 0, sizeof(map));
     bool grouped = false;
     if (p.dim != 1 && !make_block_map(&map, p, out, &grouped)) return -1;
-    const KernelRef k = dtma_kernel_for(p);
+    const KernelRef k = dtma_kernel_for(p, grouped);
     static std::mutex mu;
     static int sms[64] = {0};
-    static int occ_cache[64][2][3][3] = {};
+    static int occ_cache[64][2][3][3][2] = {};   // [device][type][dim][mode][grouped]
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return -1;
@@ -354,7 +355,7 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     {
         std::lock_guard<std::mutex> lk(mu);
         if (sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
-        int& c = occ_cache[dev][p.type][p.dim - 1][p.mode];
+        int& c = occ_cache[dev][p.type][p.dim - 1][p.mode][grouped ? 1 : 0];
         if (c == 0) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, threads, k.smem);
             if (c < 1) c = 1;

@@ -21,7 +21,10 @@
 
 namespace cuszp {
 
-template <typename T, int DIM>
+// DIRECT: grouped 2D arrays, whose codec warps write straight from registers (each store
+// instruction covers four 64-byte row pieces of whole blocks): no output buffers, so a
+// third CTA fits on an SM (measured 5.6 % faster on 8192^2 f64).
+template <typename T, int DIM, bool DIRECT = false>
 struct DecCfg {
     static constexpr int WARPS = 8;                           // codec warps
     // front warps = payload slots (1D: two -- the smaller CTA lets more of them share an
@@ -37,8 +40,10 @@ struct DecCfg {
     static constexpr int OUTW = BPW * BLK * (int)sizeof(T);   // a codec warp's decoded elements
     static constexpr int OFF_SLOT = 0;
     static constexpr int OFF_OUT = FRONT * SLOT;
-    static constexpr int BYTES = OFF_OUT + WARPS * OUTW;
+    static constexpr int BYTES = DIRECT ? OFF_OUT : OFF_OUT + WARPS * OUTW;
+    static constexpr int MIN_CTAS = DIRECT ? 3 : 2;           // per SM (register budget)
     static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }
+    static_assert(!DIRECT || DIM == 2, "direct stores are for grouped 2D arrays");
     static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
     static_assert(FRONT <= 8, "slot parities are kept in one byte");
     static_assert(DIM == 1 || BPW == (int)kGroup, "a codec warp's 2D blocks are one grouped box");
@@ -233,7 +238,7 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 
 // Decodes a codec warp's blocks of the tile in payload slot f into its output buffer
 // `ob` and starts their stores (the caller waits for the previous stores first).
-template <typename T, int DIM, int MODE, typename Src>
+template <typename T, int DIM, int MODE, bool DIRECT, typename Src>
 __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray& A, DecShared<T, DIM>& sh, int f,
                                                  int rb, int64_t lt, saddr_t pay, T* ob, saddr_t obs,
                                                  const XposeLane& xl, bool& stored, int warp, int lane)
@@ -253,10 +258,43 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
         if (lane >= o) incl += v;
     }
     const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][rb][warp] + incl - mysz;
+    const uint64_t b0 = (uint64_t)lt * C::TB + (uint64_t)warp * C::BPW;
+    if constexpr (DIRECT) {
+        // the warp's kGroup whole blocks lie in one block row (or past the array)
+        T* q = nullptr;
+        if (b0 < g.nblocks) {
+            const BlockPos p = block_pos(b0, g);
+            const uint64_t row = (uint64_t)p.z * g.dy + (uint64_t)p.y * 8 + (uint32_t)(lane >> 3);
+            q = out + row * g.dx + (uint64_t)p.x * 8 + (uint32_t)(lane & 7);
+        }
+        const uint64_t half = 4ull * g.dx;   // element l + 32 is four rows down
+#pragma unroll 1
+        for (int j = 0; j < C::BPW; j += 2) {
+            const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
+            const uint32_t rb2 = __shfl_sync(FULL, myr, j + 1), ob2 = __shfl_sync(FULL, myo, j + 1);
+            int32_t d0a, d1a, d0b, d1b;
+            decode_pair_nd<MODE>(pay, ra, rb2, oa, ob2, d0a, d1a, d0b, d1b, lane, xl);
+            if constexpr (MODE != MODE_FIXED) {
+                lorenzo_inverse<DIM>(d0a, d1a, lane);
+                lorenzo_inverse<DIM>(d0b, d1b, lane);
+            }
+            // blocks without payload decode to 0.0
+            const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb2) == 0;
+            if (q) {
+                T* qa = q + (uint32_t)j * 8;
+                qa[0] = za ? T(0) : dequant(d0a, eb);
+                qa[half] = za ? T(0) : dequant(d1a, eb);
+                qa[8] = zb ? T(0) : dequant(d0b, eb);
+                qa[8 + half] = zb ? T(0) : dequant(d1b, eb);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sh.freed[f]);   // done with the payload slot
+        return;
+    }
     // the output buffer is free once the previous stores have read it
     if (stored) bulk_wait_read();
     __syncwarp();
-    const uint64_t b0 = (uint64_t)lt * C::TB + (uint64_t)warp * C::BPW;
     if constexpr (DIM == 1) {
 #pragma unroll 1
         for (int j = 0; j < C::BPW; j += 2) {
@@ -336,11 +374,11 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
 
 // ------------------------------------------------------------------ the kernel body
 
-template <typename T, int DIM, typename Src>
+template <typename T, int DIM, bool DIRECT, typename Src>
 __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __restrict__ hdr,
                                                     unsigned long long* __restrict__ status_all)
 {
-    using C = DecCfg<T, DIM>;
+    using C = DecCfg<T, DIM, DIRECT>;
     extern __shared__ unsigned char dsm[];
     unsigned char* base = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
     uint8_t* slots = base + C::OFF_SLOT;
@@ -480,8 +518,8 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
             const int64_t lt = sh.local[f];
             const saddr_t pay = saddr(slots + f * C::SLOT);
             src.with_mode(A.mode, [&](auto m) {
-                decode_and_store<T, DIM, decltype(m)::value>(src, A, sh, f, (int)ph, lt, pay, ob, obs, xl, stored, warp,
-                                                             lane);
+                decode_and_store<T, DIM, decltype(m)::value, DIRECT>(src, A, sh, f, (int)ph, lt, pay, ob, obs, xl,
+                                                                     stored, warp, lane);
             });
             __syncwarp();
         }
@@ -491,14 +529,14 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
     finish_cta(hdr, status_all, ntotal);
 }
 
-template <typename T, int DIM, int MODE>
-__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
+template <typename T, int DIM, int MODE, bool DIRECT = false>
+__global__ void __launch_bounds__(DecCfg<T, DIM, DIRECT>::THREADS, DecCfg<T, DIM, DIRECT>::MIN_CTAS)
 decompress_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const uint8_t* __restrict__ cmp,
                       const __grid_constant__ Geom g, T eb, WsHeader* __restrict__ hdr,
                       unsigned long long* __restrict__ status, int ticket_tiles)
 {
     const SingleTiles<T, MODE> src{&tmap, out, const_cast<uint8_t*>(cmp), &g, eb, status, &hdr->total, ticket_tiles};
-    decompress_tma_body<T, DIM>(src, hdr, status);
+    decompress_tma_body<T, DIM, DIRECT>(src, hdr, status);
 }
 
 }  // namespace cuszp
