@@ -280,7 +280,7 @@ compress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* _
 }
 
 template <typename T, int DIM>
-__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, 2)
+__global__ void __launch_bounds__(DecCfg<T, DIM>::THREADS, DecCfg<T, DIM>::MIN_CTAS)
 decompress_tma_batch_kernel(const BatchItem* __restrict__ items, const uint32_t* __restrict__ tile_map,
                             const CUtensorMap* __restrict__ tmaps, uint64_t total_tiles, WsHeader* __restrict__ hdr,
                             unsigned long long* __restrict__ status, unsigned long long* __restrict__ sizes)
@@ -365,10 +365,16 @@ static size_t tma_batch_smem(bool comp)
 template <int N>
 static int fixed_threads(int, int, bool) { return N; }
 
+template <typename T>
+static int tma_threads_of(int dim, bool comp)
+{
+    if (comp) return TmaCfg<T, 1>::THREADS;   // the same for every dimension
+    return dim == 1 ? DecCfg<T, 1>::THREADS : dim == 2 ? DecCfg<T, 2>::THREADS : DecCfg<T, 3>::THREADS;
+}
+
 static int tma_threads(int type, int dim, bool comp)
 {
-    if (!comp) return dim == 1 ? DecCfg<float, 1>::THREADS : DecCfg<float, 2>::THREADS;
-    return type == 0 ? TmaCfg<float, 1>::THREADS : TmaCfg<double, 1>::THREADS;
+    return type == 0 ? tma_threads_of<float>(dim, comp) : tma_threads_of<double>(dim, comp);
 }
 
 static const void* tk(int type, int dim, bool comp)
@@ -393,10 +399,8 @@ static const Variant kVariants[] = {
     {16, 8, 4, fixed_threads<512>, false, kv<16, 8, 4>, ks<16, 8, 4>},
 };
 static_assert(TmaCfg<float, 1>::THREADS == TmaCfg<float, 3>::THREADS &&
-                  TmaCfg<double, 1>::THREADS == TmaCfg<double, 3>::THREADS &&
-                  DecCfg<float, 1>::THREADS == DecCfg<double, 1>::THREADS &&
-                  DecCfg<float, 2>::THREADS == DecCfg<double, 3>::THREADS,
-              "TMA thread counts: compress by element type, decompress by 1D or 2D/3D");
+                  TmaCfg<double, 1>::THREADS == TmaCfg<double, 3>::THREADS,
+              "TMA compress thread counts depend on the element type only");
 static_assert(TmaCfg<float, 1>::TB == 8 * 16 && TmaCfg<float, 2>::TB == 8 * 8, "TMA tiles as in variant 1");
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
