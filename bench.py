@@ -485,6 +485,21 @@ def run_serving(device, rates=(1000.0, 5000.0, 20000.0, 50000.0), count=1500, se
     return out
 
 
+def reduce_over_ranks(pg, total_s, e2e_gbs, device):
+    """The slowest rank's timed seconds (max) and end-to-end rate (min) over all ranks:
+    one all-reduce, which every rank calls."""
+    import torch
+    t = torch.tensor([total_s, -e2e_gbs], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t[0].item()), -float(t[1].item())
+
+
+def aggregate_gbs(world, input_bytes, steps, total_s):
+    """Whole-job throughput of `world` independent replicas (weak scaling): every rank's
+    input bytes over the slowest rank's time."""
+    return world * input_bytes * steps / total_s / 1e9
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -525,10 +540,7 @@ def main():
     total_s = res["total_ms"] / 1e3
     e2e_ms = res["e2e"]["value"] if "e2e" in res else 0.0
     if pg:
-        t = torch.tensor([total_s, -e2e_ms], dtype=torch.float64, device=device)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_s = float(t[0].item())
-        e2e_min = -float(t[1].item())
+        total_s, e2e_min = reduce_over_ranks(pg, total_s, e2e_ms, device)
         pg.barrier()
         pg.destroy_process_group()
     else:
@@ -538,7 +550,7 @@ def main():
     peak, kind = peaks()
     rl = roofline(res, peak, kind)
     dominant = "compress" if res["compress_ms"] >= res["decompress_ms"] else "decompress"
-    value = world * res["input_bytes"] * args.steps / total_s / 1e9
+    value = aggregate_gbs(world, res["input_bytes"], args.steps, total_s)
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
