@@ -164,6 +164,13 @@ __device__ __forceinline__ uint32_t lds_u32(saddr_t a)
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
     return v;
 }
+// 16 bytes from a 16-byte aligned shared address.
+__device__ __forceinline__ uint4 lds_u128(saddr_t a)
+{
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a) : "memory");
+    return v;
+}
 __device__ __forceinline__ void sts_val(saddr_t a, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
 __device__ __forceinline__ void sts_val(saddr_t a, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory"); }
 template <typename T> __device__ __forceinline__ T lds_val(saddr_t a);

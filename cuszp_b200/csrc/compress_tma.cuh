@@ -355,6 +355,12 @@ __device__ __forceinline__ void warp_copy_out(saddr_t src, uint32_t n, uint8_t* 
     uint8_t* first = dst - d;
     const uint32_t u0 = d ? 1u : 0u;          // first unit entirely inside [d, d + n)
     const uint32_t u1 = (d + n) >> 4;         // one past the last such unit
+    if (d == 0) {
+        // destination on a 16-byte boundary (fixed/plain 2D/3D payloads keep it so):
+        // unit u is bytes [16u, 16u + 16) of the span, one 16-byte shared load
+        for (uint32_t u = lane; u < u1; u += 32)
+            __stcs(reinterpret_cast<uint4*>(first + 16 * u), lds_u128(src + 16 * u));
+    } else
     for (uint32_t u = u0 + lane; u < u1; u += 32) {
         const uint32_t so = 16 * u - d;
         const saddr_t w = src + (so & ~3u);
