@@ -109,6 +109,29 @@ __device__ __forceinline__ void decode_pair_1d(saddr_t pay, uint32_t rA, uint32_
     const bool hasA = payload_size<1, MODE>(rA) != 0, hasB = payload_size<1, MODE>(rB) != 0;
     const uint32_t pA = oA + obA, pB = oB + obB;   // sign words
     uint32_t magA = 0, magB = 0;
+    if (nA <= 15 && nB <= 15) {
+        // the compressor's transpose carried each element's sign as plane 15 (the sign
+        // word): loading it there gives magnitudes and signs in one transpose
+        const uint32_t p = lane & 15;
+        const bool b = lane >= 16;
+        const uint32_t n = b ? nB : nA, base = b ? pB : pA;
+        uint32_t w = 0;
+        if (p < n) w = lds32<MODE>(pay, base + 4 + 4 * p);
+        else if (p == 15 && (b ? hasB : hasA)) w = lds32<MODE>(pay, base);
+        uint32_t x = 0;
+        if (hasA | hasB) x = warp_transpose32(from_stream_word(w), xl);
+        magA = x & 0x7fffu;
+        magB = (x >> 16) & 0x7fffu;
+        if constexpr (MODE == MODE_OUTLIER) {
+            if (lane == 0) {
+                if (obA) magA = ld_outlier(pay, oA, obA);
+                if (obB) magB = ld_outlier(pay, oB, obB);
+            }
+        }
+        dA = (x & 0x8000u) ? (int32_t)(0u - magA) : (int32_t)magA;
+        dB = (x & 0x80000000u) ? (int32_t)(0u - magB) : (int32_t)magB;
+        return;
+    }
     if (nA <= 16 && nB <= 16) {
         const uint32_t p = lane & 15;
         uint32_t w = 0;
@@ -171,8 +194,8 @@ __device__ __forceinline__ void decode_block_nd(saddr_t pay, uint32_t r, uint32_
     d1 = ((s1 >> lane) & 1u) ? (int32_t)(0u - mag1) : (int32_t)mag1;
 }
 
-// Two 2D/3D blocks at once: when both have payloads of rate <= 16 their transposes run
-// interleaved; otherwise one after the other.
+// Two 2D/3D blocks at once: when both have payloads of rate <= 15 their transposes run
+// interleaved (signs included); otherwise one after the other.
 template <int MODE>
 __device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_t rb, uint32_t oa, uint32_t ob_,
                                                int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane,
@@ -184,31 +207,32 @@ __device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_
         if (ra & 0x80) oba = ((ra & 0x60) >> 5) + 1;
         if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
     }
-    if (na > 16 || nb > 16 || payload_size<2, MODE>(ra) == 0 || payload_size<2, MODE>(rb) == 0) {
+    if (na > 15 || nb > 15 || payload_size<2, MODE>(ra) == 0 || payload_size<2, MODE>(rb) == 0) {
         decode_block_nd<MODE>(pay, ra, oa, d0a, d1a, lane, xl);
         decode_block_nd<MODE>(pay, rb, ob_, d0b, d1b, lane, xl);
         return;
     }
+    // lane l loads plane (l & 15) of half l >> 4, and the half's sign word in place of
+    // plane 15 (the compressor's transpose carried the signs there): one transpose per
+    // block gives magnitudes (bits 0-14, 16-30) and signs (bits 15, 31)
     const uint32_t pa = oa + oba, pb = ob_ + obb;   // sign words
     const uint32_t pl = lane & 15, h4 = (uint32_t)(lane >> 4) * 4;
-    uint32_t xa = pl < na ? lds32<MODE>(pay, pa + 8 + 8 * pl + h4) : 0u;
-    uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : 0u;
+    uint32_t xa = pl < na ? lds32<MODE>(pay, pa + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pa + h4) : 0u;
+    uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pb + h4) : 0u;
     xa = from_stream_word(xa);
     xb = from_stream_word(xb);
     warp_transpose32x2(xa, xb, xl);
-    uint32_t m0a = xa & 0xffffu, m1a = xa >> 16, m0b = xb & 0xffffu, m1b = xb >> 16;
+    uint32_t m0a = xa & 0x7fffu, m1a = (xa >> 16) & 0x7fffu, m0b = xb & 0x7fffu, m1b = (xb >> 16) & 0x7fffu;
     if constexpr (MODE == MODE_OUTLIER) {
         if (lane == 0) {
             if (oba) m0a = ld_outlier(pay, oa, oba);
             if (obb) m0b = ld_outlier(pay, ob_, obb);
         }
     }
-    const uint32_t s0a = from_stream_word(lds32<MODE>(pay, pa)), s1a = from_stream_word(lds32<MODE>(pay, pa + 4));
-    const uint32_t s0b = from_stream_word(lds32<MODE>(pay, pb)), s1b = from_stream_word(lds32<MODE>(pay, pb + 4));
-    d0a = ((s0a >> lane) & 1u) ? (int32_t)(0u - m0a) : (int32_t)m0a;
-    d1a = ((s1a >> lane) & 1u) ? (int32_t)(0u - m1a) : (int32_t)m1a;
-    d0b = ((s0b >> lane) & 1u) ? (int32_t)(0u - m0b) : (int32_t)m0b;
-    d1b = ((s1b >> lane) & 1u) ? (int32_t)(0u - m1b) : (int32_t)m1b;
+    d0a = (xa & 0x8000u) ? (int32_t)(0u - m0a) : (int32_t)m0a;
+    d1a = (xa & 0x80000000u) ? (int32_t)(0u - m1a) : (int32_t)m1a;
+    d0b = (xb & 0x8000u) ? (int32_t)(0u - m0b) : (int32_t)m0b;
+    d1b = (xb & 0x80000000u) ? (int32_t)(0u - m1b) : (int32_t)m1b;
 }
 
 // ------------------------------------------------------------------ TMA stores
