@@ -232,23 +232,33 @@ struct CompressWork {
     uint32_t wtot;
 };
 
-// Rate byte of one block from its lanes' code magnitudes (a1: 2D/3D second half).
-// 1D reduces the magnitudes as signed ints (|INT_MIN| drops out, as in the reference).
+// A block's rate byte in two steps: the warp-wide reduction of its lanes' code
+// magnitudes (a1: 2D/3D second half), then the rate arithmetic on the reduced values.
+// Split so that a warp coding several blocks can leave the second step to lane j for
+// block j, once for all its blocks.  1D reduces the magnitudes as signed ints
+// (|INT_MIN| drops out, as in the reference).
+// block_max returns the maximum magnitude -- outlier mode: without element 0, whose
+// magnitude goes to `o`.
 template <int DIM, int MODE>
-__device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lane)
+__device__ __forceinline__ uint32_t block_max(uint32_t a0, uint32_t a1, int lane, uint32_t& o)
+{
+    if constexpr (MODE == MODE_OUTLIER) {
+        o = __shfl_sync(FULL, a0, 0);
+        if constexpr (DIM == 1) return (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
+        else return __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
+    } else {
+        o = 0;
+        if constexpr (DIM == 1) return (uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0);
+        else return __reduce_max_sync(FULL, max(a0, a1));
+    }
+}
+template <int DIM, int MODE>
+__device__ __forceinline__ uint32_t rate_byte(uint32_t m2, uint32_t o)
 {
     constexpr int W = DIM == 1 ? 4 : 8;
     if constexpr (MODE == MODE_OUTLIER) {
-        // maxima without element 0 (m2) and with it (m, from m2 and element 0 itself)
-        const uint32_t o = __shfl_sync(FULL, a0, 0);
-        uint32_t m, m2;
-        if constexpr (DIM == 1) {
-            m2 = (uint32_t)max(__reduce_max_sync(FULL, lane ? (int)a0 : 0), 0);
-            m = (uint32_t)max((int)m2, (int)o);
-        } else {
-            m2 = __reduce_max_sync(FULL, lane ? max(a0, a1) : a1);
-            m = max(m2, o);
-        }
+        // m2: maximum without element 0; m: with it
+        const uint32_t m = DIM == 1 ? (uint32_t)max((int)m2, (int)o) : max(m2, o);
         const int fr1 = bitlen(m);
         const int fr2 = bitlen(m2);
         const int ob = (bitlen(o) + 7) / 8;
@@ -256,9 +266,15 @@ __device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lan
         const int cost2 = fr2 ? W + fr2 * W + ob : W + ob;
         return cost1 <= cost2 ? (uint32_t)fr1 : (uint32_t)((fr2 | 0x80 | ((ob - 1) << 5)) & 0xff);
     } else {
-        if constexpr (DIM == 1) return (uint32_t)bitlen((uint32_t)max(__reduce_max_sync(FULL, (int)a0), 0));
-        else return (uint32_t)bitlen(__reduce_max_sync(FULL, max(a0, a1)));
+        return (uint32_t)bitlen(m2);
     }
+}
+template <int DIM, int MODE>
+__device__ __forceinline__ uint32_t block_rate(uint32_t a0, uint32_t a1, int lane)
+{
+    uint32_t o;
+    const uint32_t m = block_max<DIM, MODE>(a0, a1, lane, o);
+    return rate_byte<DIM, MODE>(m, o);
 }
 
 // Plane-word stores.  Blocks of rate <= 15 (the common case) carry each element's
@@ -321,7 +337,9 @@ __device__ __forceinline__ void pack_pair_1d(uint32_t rA, uint32_t rB, int32_t c
 }
 
 // Payload of one 2D/3D block (rate r != 0; codes c0, c1 of this lane's two elements) at p.
-template <int MODE>
+// HEAD: outlier mode, the caller has written element 0's bytes, zeroed its magnitude
+// (sign kept) and passes p past them.
+template <int MODE, bool HEAD = false>
 __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1, saddr_t p, int lane,
                                               const XposeLane& xl)
 {
@@ -332,7 +350,7 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
     }
     uint32_t a0 = uabs(c0);
     const uint32_t a1 = uabs(c1);
-    if constexpr (MODE == MODE_OUTLIER) {
+    if constexpr (MODE == MODE_OUTLIER && !HEAD) {
         // element 0's magnitude, little-endian, one byte per lane
         const uint32_t o = __shfl_sync(FULL, a0, 0);
         if ((uint32_t)lane < ob) sts_u8(p + lane, o >> (8 * lane));
@@ -365,7 +383,8 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
 // Payloads of two 2D/3D blocks a and b (rates ra, rb) at pa / pb; both blocks'
 // transposes run interleaved when both rates are <= 15.  NARROW: the caller knows
 // both rates are <= 15 (no fallback branch, so consecutive pairs can interleave).
-template <int MODE, bool NARROW = false>
+// HEAD: as for pack_block_nd.
+template <int MODE, bool NARROW = false, bool HEAD = false>
 __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c0a, int32_t c1a, int32_t c0b,
                                              int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
 {
@@ -376,13 +395,13 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
         if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
     }
     if (!NARROW && (na > 15 || nb > 15)) {
-        if (ra) pack_block_nd<MODE>(ra, c0a, c1a, pa, lane, xl);
-        if (rb) pack_block_nd<MODE>(rb, c0b, c1b, pb, lane, xl);
+        if (ra) pack_block_nd<MODE, HEAD>(ra, c0a, c1a, pa, lane, xl);
+        if (rb) pack_block_nd<MODE, HEAD>(rb, c0b, c1b, pb, lane, xl);
         return;
     }
     uint32_t a0a = uabs(c0a), a0b = uabs(c0b);
     const uint32_t a1a = uabs(c1a), a1b = uabs(c1b);
-    if constexpr (MODE == MODE_OUTLIER) {
+    if constexpr (MODE == MODE_OUTLIER && !HEAD) {
         // element 0's magnitude, little-endian, one byte per lane (lanes 0-3: a, 4-7: b)
         const uint32_t oa = __shfl_sync(FULL, a0a, 0), ob = __shfl_sync(FULL, a0b, 0);
         const uint32_t i = lane & 3;

@@ -201,6 +201,7 @@ struct WarpCodes {
     int32_t c0[C::BPW];
     int32_t c1[DIM == 1 ? 1 : C::BPW];
     uint32_t rb;   // lane j < BPW: rate byte of block j
+    uint32_t o;    // 2D/3D outlier mode, lane j < BPW: magnitude of block j's element 0
 };
 
 // 1D code phase: the warp's 16 blocks of tile `t` (elements in `tin`) -> codes, rate
@@ -210,8 +211,7 @@ __device__ __forceinline__ uint32_t codes_1d(saddr_t tin, WarpCodes<1, C>& K, in
                                              T recip, uint8_t* __restrict__ cmp, int lane)
 {
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-    uint32_t off = 0;
-    K.rb = 0;
+    uint32_t M = 0, O = 0;   // lane j: block j's reduced magnitudes
     const saddr_t wb = tin + (warp * C::BPW * 32 + lane) * (uint32_t)sizeof(T);
     const bool ragged = (b0 + C::BPW) * 32 > g.nbEle;   // also: no element at all
 #pragma unroll
@@ -231,14 +231,15 @@ __device__ __forceinline__ uint32_t codes_1d(saddr_t tin, WarpCodes<1, C>& K, in
         }
         K.c0[j] = cA;
         K.c0[j + 1] = cB;
-        const uint32_t rA = block_rate<1, MODE>(uabs(cA), 0u, lane);
-        const uint32_t rB = block_rate<1, MODE>(uabs(cB), 0u, lane);
-        if (lane == j) K.rb = rA;
-        if (lane == j + 1) K.rb = rB;
-        off += payload_size<1, MODE>(rA) + payload_size<1, MODE>(rB);
+        uint32_t oA, oB;
+        const uint32_t mA = block_max<1, MODE>(uabs(cA), 0u, lane, oA);
+        const uint32_t mB = block_max<1, MODE>(uabs(cB), 0u, lane, oB);
+        if (lane == j) { M = mA; O = oA; }
+        if (lane == j + 1) { M = mB; O = oB; }
     }
+    K.rb = lane < C::BPW ? rate_byte<1, MODE>(M, O) : 0u;
     if (lane < C::BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)K.rb;
-    return off;
+    return __reduce_add_sync(FULL, payload_size<1, MODE>(K.rb));
 }
 
 // 2D/3D code phase: the warp's 8 blocks (each block's 64 elements contiguous in `tin`).
@@ -249,8 +250,6 @@ __device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, 
     constexpr uint32_t B = DIM == 2 ? 8 : 4;
     static_assert(C::BPW % 4 == 0, "blocks are coded four at a time");
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-    uint32_t off = 0;
-    K.rb = 0;
     const saddr_t wb = tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);   // this lane's element
     const uint32_t nblk = b0 < g.nblocks ? (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0) : 0u;
     // partial blocks exist only along axes the block size does not divide
@@ -296,14 +295,28 @@ __device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, 
             }
         }
     }
+    // per block one reduction; lane j then derives block j's rate byte
+    uint32_t M = 0, O = 0;
 #pragma unroll
     for (int j = 0; j < C::BPW; j++) {
-        const uint32_t r = block_rate<DIM, MODE>(uabs(K.c0[j]), uabs(K.c1[j]), lane);
-        if (lane == j) K.rb = r;
-        off += payload_size<DIM, MODE>(r);
+        uint32_t o;
+        const uint32_t m = block_max<DIM, MODE>(uabs(K.c0[j]), uabs(K.c1[j]), lane, o);
+        if (lane == j) { M = m; O = o; }
+    }
+    K.rb = lane < C::BPW ? rate_byte<DIM, MODE>(M, O) : 0u;
+    if constexpr (MODE == MODE_OUTLIER) {
+        // element 0 of a block flagged as outlier goes ahead of its planes in whole bytes
+        // (written by the pack phase from K.o); its planes carry magnitude 0, sign kept
+        K.o = O;
+        const uint32_t head = __ballot_sync(FULL, K.rb & 0x80u);
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < C::BPW; j++)
+                if ((head >> j) & 1u) K.c0[j] = (int32_t)((uint32_t)K.c0[j] & 0x80000000u);
+        }
     }
     if (lane < C::BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)K.rb;
-    return off;
+    return __reduce_add_sync(FULL, payload_size<DIM, MODE>(K.rb));
 }
 
 // Pack phase: sign maps and bit-planes of the warp's blocks, in stream order at `out`.
@@ -318,8 +331,20 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
         const uint32_t v = __shfl_up_sync(FULL, incl, o);
         if (lane >= o) incl += v;
     }
-    const uint32_t myoff = incl - sz;
+    uint32_t myoff = incl - sz;
     if constexpr (DIM != 1) {
+        if constexpr (MODE == MODE_OUTLIER) {
+            // element 0's bytes of every outlier block at once: lane 4j + i writes byte i of
+            // block j; the planes then start past them (myoff: block j's sign words)
+            static_assert(4 * C::BPW <= 32, "four lanes per block");
+            const uint32_t ob = (mine & 0x80u) ? ((mine & 0x60u) >> 5) + 1u : 0u;
+            const int src = lane >> 2;
+            const uint32_t i = lane & 3;
+            const uint32_t n = __shfl_sync(FULL, ob, src), v = __shfl_sync(FULL, K.o, src);
+            const uint32_t at = __shfl_sync(FULL, myoff, src);
+            if (i < n) sts_u8(out + at + i, v >> (8 * i));
+            myoff += ob;
+        }
         const uint32_t n = MODE == MODE_OUTLIER ? (mine & 0x1fu) : mine;
         if (__all_sync(FULL, n <= 15)) {
             // every block narrow: all pairs unrolled, no branches between them
@@ -327,8 +352,8 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
             for (int j = 0; j < C::BPW; j += 2) {
                 const uint32_t ra = __shfl_sync(FULL, mine, j), rb = __shfl_sync(FULL, mine, j + 1);
                 const uint32_t oa = __shfl_sync(FULL, myoff, j), ob = __shfl_sync(FULL, myoff, j + 1);
-                pack_pair_nd<MODE, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane,
-                                         xl);
+                pack_pair_nd<MODE, true, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob,
+                                               lane, xl);
             }
             return;
         }
@@ -341,7 +366,8 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
         if constexpr (DIM == 1)
             pack_pair_1d<MODE>(ra, rb, K.c0[j], K.c0[j + 1], out + oa, out + ob, lane, xl);
         else
-            pack_pair_nd<MODE>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane, xl);
+            pack_pair_nd<MODE, false, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob,
+                                            lane, xl);
     }
 }
 
