@@ -108,6 +108,9 @@ SHAPES = [
     (3, (4, 1, 1), None),
     (3, (68, 37, 29), None),
     (3, (256, 130, 66), None),
+    # block rows of whole codec warps (dims.x % 32 == 0): f32 decompress stores one
+    # x-fastest box per warp; 40 blocks per row, so tiles span rows; ragged y and z
+    (3, (160, 22, 11), None),
 ]
 
 
