@@ -194,6 +194,37 @@ __device__ __forceinline__ void decode_block_nd(saddr_t pay, uint32_t r, uint32_
     d1 = ((s1 >> lane) & 1u) ? (int32_t)(0u - mag1) : (int32_t)mag1;
 }
 
+// Two 2D/3D blocks with payloads of rate <= 15 (na, nb planes; sign words at pa / pb),
+// their transposes interleaved.  Lane l loads plane (l & 15) of half l >> 4, and the
+// half's sign word in place of plane 15 (the compressor's transpose carried the signs
+// there): one transpose per block gives magnitudes (bits 0-14, 16-30) and signs (bits
+// 15, 31).  Outlier mode: ha / hb tell whether element 0's magnitude is stored ahead of
+// the planes; it is ma / mb then (read by lane 0 only).
+template <int MODE>
+__device__ __forceinline__ void decode_pair_narrow(saddr_t pay, uint32_t pa, uint32_t pb, uint32_t na, uint32_t nb,
+                                                   bool ha, bool hb, uint32_t ma, uint32_t mb, int32_t& d0a,
+                                                   int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane,
+                                                   const XposeLane& xl)
+{
+    const uint32_t pl = lane & 15, h4 = (uint32_t)(lane >> 4) * 4;
+    uint32_t xa = pl < na ? lds32<MODE>(pay, pa + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pa + h4) : 0u;
+    uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pb + h4) : 0u;
+    xa = from_stream_word(xa);
+    xb = from_stream_word(xb);
+    warp_transpose32x2(xa, xb, xl);
+    uint32_t m0a = xa & 0x7fffu, m1a = (xa >> 16) & 0x7fffu, m0b = xb & 0x7fffu, m1b = (xb >> 16) & 0x7fffu;
+    if constexpr (MODE == MODE_OUTLIER) {
+        if (lane == 0) {
+            if (ha) m0a = ma;
+            if (hb) m0b = mb;
+        }
+    }
+    d0a = (xa & 0x8000u) ? (int32_t)(0u - m0a) : (int32_t)m0a;
+    d1a = (xa & 0x80000000u) ? (int32_t)(0u - m1a) : (int32_t)m1a;
+    d0b = (xb & 0x8000u) ? (int32_t)(0u - m0b) : (int32_t)m0b;
+    d1b = (xb & 0x80000000u) ? (int32_t)(0u - m1b) : (int32_t)m1b;
+}
+
 // Two 2D/3D blocks at once: when both have payloads of rate <= 15 their transposes run
 // interleaved (signs included); otherwise one after the other.
 template <int MODE>
@@ -212,27 +243,15 @@ __device__ __forceinline__ void decode_pair_nd(saddr_t pay, uint32_t ra, uint32_
         decode_block_nd<MODE>(pay, rb, ob_, d0b, d1b, lane, xl);
         return;
     }
-    // lane l loads plane (l & 15) of half l >> 4, and the half's sign word in place of
-    // plane 15 (the compressor's transpose carried the signs there): one transpose per
-    // block gives magnitudes (bits 0-14, 16-30) and signs (bits 15, 31)
-    const uint32_t pa = oa + oba, pb = ob_ + obb;   // sign words
-    const uint32_t pl = lane & 15, h4 = (uint32_t)(lane >> 4) * 4;
-    uint32_t xa = pl < na ? lds32<MODE>(pay, pa + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pa + h4) : 0u;
-    uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pb + h4) : 0u;
-    xa = from_stream_word(xa);
-    xb = from_stream_word(xb);
-    warp_transpose32x2(xa, xb, xl);
-    uint32_t m0a = xa & 0x7fffu, m1a = (xa >> 16) & 0x7fffu, m0b = xb & 0x7fffu, m1b = (xb >> 16) & 0x7fffu;
+    uint32_t ma = 0, mb = 0;
     if constexpr (MODE == MODE_OUTLIER) {
         if (lane == 0) {
-            if (oba) m0a = ld_outlier(pay, oa, oba);
-            if (obb) m0b = ld_outlier(pay, ob_, obb);
+            if (oba) ma = ld_outlier(pay, oa, oba);
+            if (obb) mb = ld_outlier(pay, ob_, obb);
         }
     }
-    d0a = (xa & 0x8000u) ? (int32_t)(0u - m0a) : (int32_t)m0a;
-    d1a = (xa & 0x80000000u) ? (int32_t)(0u - m1a) : (int32_t)m1a;
-    d0b = (xb & 0x8000u) ? (int32_t)(0u - m0b) : (int32_t)m0b;
-    d1b = (xb & 0x80000000u) ? (int32_t)(0u - m1b) : (int32_t)m1b;
+    decode_pair_narrow<MODE>(pay, oa + oba, ob_ + obb, na, nb, oba != 0, obb != 0, ma, mb, d0a, d1a, d0b, d1b, lane,
+                             xl);
 }
 
 // ------------------------------------------------------------------ TMA stores
@@ -285,6 +304,42 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
     }
     const uint32_t myo = bad ? 0u : sh.poff[f] + sh.woff[f][rb][warp] + incl - mysz;
     const uint64_t b0 = (uint64_t)lt * C::TB + (uint64_t)warp * C::BPW;
+    // 2D/3D: lane j derives block j's plane count, sign-word offset and (outlier mode)
+    // element 0's magnitude once; a warp whose blocks all have payloads of rate <= 15
+    // then decodes every pair on the narrow path without per-pair rate arithmetic
+    uint32_t myn = myr, myps = myo, mym = 0, heads = 0;
+    bool narrow = false;
+    if constexpr (DIM != 1) {
+        if constexpr (MODE == MODE_OUTLIER) {
+            myn = myr & 0x1fu;
+            const uint32_t myob = (myr & 0x80u) ? ((myr & 0x60u) >> 5) + 1u : 0u;
+            if (myob) mym = ld_outlier(pay, myo, myob);
+            myps = myo + myob;
+            heads = __ballot_sync(FULL, myob != 0);
+        }
+        narrow = __all_sync(FULL, lane >= C::BPW || (mysz != 0 && myn <= 15));
+    }
+    auto decode = [&](int j, int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, bool& za, bool& zb) {
+        if (narrow) {
+            const uint32_t pa = __shfl_sync(FULL, myps, j), pb = __shfl_sync(FULL, myps, j + 1);
+            const uint32_t na = __shfl_sync(FULL, myn, j), nb = __shfl_sync(FULL, myn, j + 1);
+            uint32_t ma = 0, mb = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                ma = __shfl_sync(FULL, mym, j);
+                mb = __shfl_sync(FULL, mym, j + 1);
+            }
+            decode_pair_narrow<MODE>(pay, pa, pb, na, nb, (heads >> j) & 1u, (heads >> (j + 1)) & 1u, ma, mb, d0a,
+                                     d1a, d0b, d1b, lane, xl);
+            za = zb = false;
+        } else {
+            const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
+            const uint32_t rb2 = __shfl_sync(FULL, myr, j + 1), ob2 = __shfl_sync(FULL, myo, j + 1);
+            decode_pair_nd<MODE>(pay, ra, rb2, oa, ob2, d0a, d1a, d0b, d1b, lane, xl);
+            // blocks without payload decode to 0.0
+            za = payload_size<DIM, MODE>(ra) == 0;
+            zb = payload_size<DIM, MODE>(rb2) == 0;
+        }
+    };
     if constexpr (DIRECT) {
         // the warp's kGroup whole blocks lie in one block row (or past the array)
         T* q = nullptr;
@@ -296,16 +351,13 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
         const uint64_t half = 4ull * g.dx;   // element l + 32 is four rows down
 #pragma unroll 1
         for (int j = 0; j < C::BPW; j += 2) {
-            const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
-            const uint32_t rb2 = __shfl_sync(FULL, myr, j + 1), ob2 = __shfl_sync(FULL, myo, j + 1);
             int32_t d0a, d1a, d0b, d1b;
-            decode_pair_nd<MODE>(pay, ra, rb2, oa, ob2, d0a, d1a, d0b, d1b, lane, xl);
+            bool za, zb;
+            decode(j, d0a, d1a, d0b, d1b, za, zb);
             if constexpr (MODE != MODE_FIXED) {
                 lorenzo_inverse<DIM>(d0a, d1a, lane);
                 lorenzo_inverse<DIM>(d0b, d1b, lane);
             }
-            // blocks without payload decode to 0.0
-            const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb2) == 0;
             if (q) {
                 T* qa = q + (uint32_t)j * 8;
                 qa[0] = za ? T(0) : dequant(d0a, eb);
@@ -340,15 +392,13 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
     } else {
 #pragma unroll 1
         for (int j = 0; j < C::BPW; j += 2) {
-            const uint32_t ra = __shfl_sync(FULL, myr, j), oa = __shfl_sync(FULL, myo, j);
-            const uint32_t rb = __shfl_sync(FULL, myr, j + 1), obo = __shfl_sync(FULL, myo, j + 1);
             int32_t d0a, d1a, d0b, d1b;
-            decode_pair_nd<MODE>(pay, ra, rb, oa, obo, d0a, d1a, d0b, d1b, lane, xl);
+            bool za, zb;
+            decode(j, d0a, d1a, d0b, d1b, za, zb);
             if constexpr (MODE != MODE_FIXED) {
                 lorenzo_inverse<DIM>(d0a, d1a, lane);
                 lorenzo_inverse<DIM>(d0b, d1b, lane);
             }
-            const bool za = payload_size<DIM, MODE>(ra) == 0, zb = payload_size<DIM, MODE>(rb) == 0;
             const saddr_t oj = obs + j * 64 * sizeof(T);
             sts_val(oj, za ? T(0) : dequant(d0a, eb));
             sts_val(oj + 32 * sizeof(T), za ? T(0) : dequant(d1a, eb));
