@@ -44,7 +44,8 @@ __device__ __forceinline__ void put32s(saddr_t a, uint32_t v)
             sts_u16(a, v);
             sts_u16(a + 2, v >> 16);
         } else {
-            sts_u8(a, v); sts_u8(a + 1, v >> 8); sts_u8(a + 2, v >> 16); sts_u8(a + 3, v >> 24);
+            // odd offset: the middle two bytes are a 2-byte aligned pair
+            sts_u8(a, v); sts_u16(a + 1, v >> 8); sts_u8(a + 3, v >> 24);
         }
     } else {
         sts_u32(a, v);
@@ -380,11 +381,35 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
     }
 }
 
+// Payloads of two 2D/3D blocks of rate <= 15, sign words at pa / pb, transposes
+// interleaved.  Lane l holds plane (l ^ 7) & 15 of half l >> 4 after the transpose
+// (plane 15 = the half's signs) and stores it when that bit of the block's plane mask
+// is set (ka / kb: bits 0 .. n-1 and 15 for a block with a payload, 0 without).  In
+// outlier mode element 0's magnitude must already be cleared (sign kept) where the
+// block stores element 0 ahead of its planes.
+template <int MODE>
+__device__ __forceinline__ void pack_pair_narrow(uint32_t ka, uint32_t kb, int32_t c0a, int32_t c1a, int32_t c0b,
+                                                 int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
+{
+    const uint32_t a0a = uabs(c0a), a0b = uabs(c0b), a1a = uabs(c1a), a1b = uabs(c1b);
+    uint32_t xa = (a0a & 0x7fffu) | ((a1a << 16) & 0x7fff0000u) | (((uint32_t)c0a >> 16) & 0x8000u) |
+                  ((uint32_t)c1a & 0x80000000u);
+    uint32_t xb = (a0b & 0x7fffu) | ((a1b << 16) & 0x7fff0000u) | (((uint32_t)c0b >> 16) & 0x8000u) |
+                  ((uint32_t)c1b & 0x80000000u);
+    warp_transpose32x2(xa, xb, xl);
+    const uint32_t pl = (lane ^ 7) & 15;
+    const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
+    const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
+    if ((ka >> pl) & 1u) put32s<MODE>(pa + o, xa);
+    if ((kb >> pl) & 1u) put32s<MODE>(pb + o, xb);
+}
+
+// Plane mask of a block for pack_pair_narrow (rate byte r, n <= 15 planes).
+__device__ __forceinline__ uint32_t plane_mask(uint32_t r, uint32_t n) { return r ? ((1u << n) - 1u) | 0x8000u : 0u; }
+
 // Payloads of two 2D/3D blocks a and b (rates ra, rb) at pa / pb; both blocks'
-// transposes run interleaved when both rates are <= 15.  NARROW: the caller knows
-// both rates are <= 15 (no fallback branch, so consecutive pairs can interleave).
-// HEAD: as for pack_block_nd.
-template <int MODE, bool NARROW = false, bool HEAD = false>
+// transposes run interleaved when both rates are <= 15.  HEAD: as for pack_block_nd.
+template <int MODE, bool HEAD = false>
 __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c0a, int32_t c1a, int32_t c0b,
                                              int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
 {
@@ -394,36 +419,24 @@ __device__ __forceinline__ void pack_pair_nd(uint32_t ra, uint32_t rb, int32_t c
         if (ra & 0x80) oba = ((ra & 0x60) >> 5) + 1;
         if (rb & 0x80) obb = ((rb & 0x60) >> 5) + 1;
     }
-    if (!NARROW && (na > 15 || nb > 15)) {
+    if (na > 15 || nb > 15) {
         if (ra) pack_block_nd<MODE, HEAD>(ra, c0a, c1a, pa, lane, xl);
         if (rb) pack_block_nd<MODE, HEAD>(rb, c0b, c1b, pb, lane, xl);
         return;
     }
-    uint32_t a0a = uabs(c0a), a0b = uabs(c0b);
-    const uint32_t a1a = uabs(c1a), a1b = uabs(c1b);
     if constexpr (MODE == MODE_OUTLIER && !HEAD) {
         // element 0's magnitude, little-endian, one byte per lane (lanes 0-3: a, 4-7: b)
-        const uint32_t oa = __shfl_sync(FULL, a0a, 0), ob = __shfl_sync(FULL, a0b, 0);
+        const uint32_t oa = __shfl_sync(FULL, uabs(c0a), 0), ob = __shfl_sync(FULL, uabs(c0b), 0);
         const uint32_t i = lane & 3;
         if (lane < 4 && i < oba) sts_u8(pa + i, oa >> (8 * i));
         if (lane >= 4 && lane < 8 && i < obb) sts_u8(pb + i, ob >> (8 * i));
-        if (lane == 0) {
-            if (oba) a0a = 0;
-            if (obb) a0b = 0;
+        if (lane == 0) {   // magnitude 0 in the planes, sign kept
+            if (oba) c0a = (int32_t)((uint32_t)c0a & 0x80000000u);
+            if (obb) c0b = (int32_t)((uint32_t)c0b & 0x80000000u);
         }
         pa += oba; pb += obb;
     }
-    // lane l holds plane (l ^ 7) & 15 of half l >> 4; plane 15 = the half's signs
-    uint32_t xa = (a0a & 0x7fffu) | ((a1a << 16) & 0x7fff0000u) | (((uint32_t)c0a >> 16) & 0x8000u) |
-                  ((uint32_t)c1a & 0x80000000u);
-    uint32_t xb = (a0b & 0x7fffu) | ((a1b << 16) & 0x7fff0000u) | (((uint32_t)c0b >> 16) & 0x8000u) |
-                  ((uint32_t)c1b & 0x80000000u);
-    warp_transpose32x2(xa, xb, xl);
-    const uint32_t pl = (lane ^ 7) & 15;
-    const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
-    const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
-    if (ra && (pl == 15 || pl < na)) put32s<MODE>(pa + o, xa);
-    if (rb && (pl == 15 || pl < nb)) put32s<MODE>(pb + o, xb);
+    pack_pair_narrow<MODE>(plane_mask(ra, na), plane_mask(rb, nb), c0a, c1a, c0b, c1b, pa, pb, lane, xl);
 }
 
 // Sign maps and bit-planes of the warp's blocks at their final offsets.

@@ -347,13 +347,15 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
         }
         const uint32_t n = MODE == MODE_OUTLIER ? (mine & 0x1fu) : mine;
         if (__all_sync(FULL, n <= 15)) {
-            // every block narrow: all pairs unrolled, no branches between them
+            // every block narrow: all pairs unrolled, no branches between them; lane j
+            // holds block j's plane mask
+            const uint32_t mask = plane_mask(mine, n);
 #pragma unroll
             for (int j = 0; j < C::BPW; j += 2) {
-                const uint32_t ra = __shfl_sync(FULL, mine, j), rb = __shfl_sync(FULL, mine, j + 1);
+                const uint32_t ka = __shfl_sync(FULL, mask, j), kb = __shfl_sync(FULL, mask, j + 1);
                 const uint32_t oa = __shfl_sync(FULL, myoff, j), ob = __shfl_sync(FULL, myoff, j + 1);
-                pack_pair_nd<MODE, true, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob,
-                                               lane, xl);
+                pack_pair_narrow<MODE>(ka, kb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane,
+                                       xl);
             }
             return;
         }
@@ -366,8 +368,8 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
         if constexpr (DIM == 1)
             pack_pair_1d<MODE>(ra, rb, K.c0[j], K.c0[j + 1], out + oa, out + ob, lane, xl);
         else
-            pack_pair_nd<MODE, false, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob,
-                                            lane, xl);
+            pack_pair_nd<MODE, true>(ra, rb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane,
+                                     xl);
     }
 }
 
