@@ -206,9 +206,12 @@ __device__ __forceinline__ void decode_pair_narrow(saddr_t pay, uint32_t pa, uin
                                                    int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane,
                                                    const XposeLane& xl)
 {
+    // one load per lane and block: its plane word, or in slot 15 the sign word
     const uint32_t pl = lane & 15, h4 = (uint32_t)(lane >> 4) * 4;
-    uint32_t xa = pl < na ? lds32<MODE>(pay, pa + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pa + h4) : 0u;
-    uint32_t xb = pl < nb ? lds32<MODE>(pay, pb + 8 + 8 * pl + h4) : pl == 15 ? lds32<MODE>(pay, pb + h4) : 0u;
+    const uint32_t op = 8 + 8 * pl + h4;
+    const uint32_t oa = pl < na ? op : h4, ob = pl < nb ? op : h4;
+    uint32_t xa = (pl < na || pl == 15) ? lds32<MODE>(pay, pa + oa) : 0u;
+    uint32_t xb = (pl < nb || pl == 15) ? lds32<MODE>(pay, pb + ob) : 0u;
     xa = from_stream_word(xa);
     xb = from_stream_word(xb);
     warp_transpose32x2(xa, xb, xl);
