@@ -262,6 +262,28 @@ __device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, con
         b = (b & xl.keep[i]) | (__funnelshift_r(yb, yb, xl.rot[i]) & ~xl.keep[i]);
     }
 }
+// Two transposes of stream-order words, for the decoder: lane l holds the word of row
+// (l ^ 7), whose bit (e ^ 7) is column e (the reference's byte order, 8 columns per byte,
+// first one in the most significant bit); on exit lane p holds column p with bit r =
+// row r, so no per-word byte-order conversion is needed.  It is the butterfly of
+// XposeLane(lane ^ 7), which swaps the keep / rotate roles of the three sub-byte stages:
+// those stages keep ~keep and rotate the other way, from the same XposeLane(lane).
+__device__ __forceinline__ void warp_transpose32x2_stream(uint32_t& a, uint32_t& b, const XposeLane& xl)
+{
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        const int j = 16 >> i;
+        const uint32_t ya = __shfl_xor_sync(FULL, a, j);
+        const uint32_t yb = __shfl_xor_sync(FULL, b, j);
+        if (i < 2) {
+            a = (a & xl.keep[i]) | (__funnelshift_r(ya, ya, xl.rot[i]) & ~xl.keep[i]);
+            b = (b & xl.keep[i]) | (__funnelshift_r(yb, yb, xl.rot[i]) & ~xl.keep[i]);
+        } else {
+            a = (a & ~xl.keep[i]) | (__funnelshift_l(ya, ya, xl.rot[i]) & xl.keep[i]);
+            b = (b & ~xl.keep[i]) | (__funnelshift_l(yb, yb, xl.rot[i]) & xl.keep[i]);
+        }
+    }
+}
 __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, const XposeLane& xl)
 {
 #pragma unroll

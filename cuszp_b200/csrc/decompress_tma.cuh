@@ -206,15 +206,15 @@ __device__ __forceinline__ void decode_pair_narrow(saddr_t pay, uint32_t pa, uin
                                                    int32_t& d1a, int32_t& d0b, int32_t& d1b, int lane,
                                                    const XposeLane& xl)
 {
-    // one load per lane and block: its plane word, or in slot 15 the sign word
-    const uint32_t pl = lane & 15, h4 = (uint32_t)(lane >> 4) * 4;
+    // one load per lane and block: lane l takes plane (l ^ 7) & 15 of half l >> 4, or in
+    // slot 15 the half's sign word, as stored; the stream-order transpose (xl: this
+    // lane's XposeLane(lane)) then leaves element p's planes in bits 0-14 / 16-30 of lane p
+    const uint32_t pl = (uint32_t)(lane ^ 7) & 15, h4 = (uint32_t)(lane >> 4) * 4;
     const uint32_t op = 8 + 8 * pl + h4;
     const uint32_t oa = pl < na ? op : h4, ob = pl < nb ? op : h4;
     uint32_t xa = (pl < na || pl == 15) ? lds32<MODE>(pay, pa + oa) : 0u;
     uint32_t xb = (pl < nb || pl == 15) ? lds32<MODE>(pay, pb + ob) : 0u;
-    xa = from_stream_word(xa);
-    xb = from_stream_word(xb);
-    warp_transpose32x2(xa, xb, xl);
+    warp_transpose32x2_stream(xa, xb, xl);
     uint32_t m0a = xa & 0x7fffu, m1a = (xa >> 16) & 0x7fffu, m0b = xb & 0x7fffu, m1b = (xb >> 16) & 0x7fffu;
     if constexpr (MODE == MODE_OUTLIER) {
         if (lane == 0) {
