@@ -215,24 +215,6 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int row)
     return x;
 }
 
-// Two independent transposes, interleaved stage by stage (twice the work per
-// dependent step of the butterfly).
-__device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, int row)
-{
-#pragma unroll
-    for (int j = 16; j >= 1; j >>= 1) {
-        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
-                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
-        const uint32_t ya = __shfl_xor_sync(FULL, a, j);
-        const uint32_t yb = __shfl_xor_sync(FULL, b, j);
-        const bool up = row & j;
-        const uint32_t keep = up ? m : ~m;
-        const int rot = up ? j : 32 - j;
-        a = (a & keep) | (__funnelshift_r(ya, ya, rot) & ~keep);
-        b = (b & keep) | (__funnelshift_r(yb, yb, rot) & ~keep);
-    }
-}
-
 // The per-lane constants of the five butterfly stages for a fixed row index, for loops
 // that transpose many words with the same row: keep mask and rotate amount per stage.
 struct XposeLane {
@@ -251,6 +233,8 @@ struct XposeLane {
         }
     }
 };
+// Two independent transposes, interleaved stage by stage (twice the work per dependent
+// step of the butterfly).
 __device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, const XposeLane& xl)
 {
 #pragma unroll
