@@ -49,7 +49,9 @@ WORKLOADS = {
                                  (1, 8192, 8192), "abs", 1e-3, "uni"),
 }
 DEFAULT = "grf512_f32_outlier_3d"
-ALSO = ["uniform8192_f64_fixed_2d", "sinusoid_f32_plain_1d"]
+ALSO = ["uniform8192_f64_fixed_2d", "sinusoid_f32_plain_1d", "grf512_f32_outlier_2d", "grf512_f32_outlier_1d"]
+L2_BYTES = 126 << 20          # B200 L2
+FLUSH_BYTES = 256 << 20       # written between kernels when a workload's arrays could stay in L2
 
 
 def peaks():
@@ -206,6 +208,9 @@ def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
     size = torch.zeros(1, dtype=torch.int64, device=device)
     ws = codec.Workspace(device)
     ws.ensure(codec.workspace_size(lay, x.dtype, mode))
+    # arrays that fit in L2 (input + stream + output): flush it before every kernel, outside
+    # the timed brackets, so each kernel reads its inputs from HBM
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device) if 3 * nbytes < 2 * L2_BYTES else None
 
     def step():
         codec.compress_into(x, cmp, eb, mode, dim, lay.dims, size_out=size, stream=stream, workspace=ws)
@@ -218,7 +223,7 @@ def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
     ws.check(stream)
     S = int(size.item())
 
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
     return_clock = None
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
@@ -226,18 +231,27 @@ def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
     with ClockSampler(device) as clk:
         t0.record(stream)
         for i in range(steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.fill_(i & 0xff)
             ev[i][0].record(stream)
             codec.compress_into(x, cmp, eb, mode, dim, lay.dims, size_out=size, stream=stream, workspace=ws)
             ev[i][1].record(stream)
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.fill_((i + 1) & 0xff)
+                ev[i][3].record(stream)
             codec.decompress_into(cmp, out, eb, mode, dim, lay.dims, stream=stream, workspace=ws)
             ev[i][2].record(stream)
         t1.record(stream)
         torch.cuda.synchronize()
     return_clock = clk.summary()
     ws.check(stream)
-    total_ms = t0.elapsed_time(t1)
     c_ms = [e[0].elapsed_time(e[1]) for e in ev]
-    d_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    d_ms = [e[3 if flush is not None else 1].elapsed_time(e[2]) for e in ev]
+    # with flushes the step time is the kernels' time alone
+    total_ms = t0.elapsed_time(t1) if flush is None else sum(c_ms) + sum(d_ms)
+    del flush
 
     # correctness of what was timed: FP64 error check on the device
     err = (x.double() - out.double()).abs()
@@ -254,6 +268,8 @@ def run_workload(name, steps, warmup, device, stream, rank=0, measure_e2e=True):
         "compress_ms_min": min(c_ms), "decompress_ms_min": min(d_ms),
         "over_eb": over_eb, "over_1.1eb": over_11, "max_err_over_eb": maxerr / ebd if ebd else None,
         "clocks": return_clock, "launches": 2 * steps,
+        "l2": "L2 flushed (256 MiB write) before every kernel, outside the timed brackets" if 3 * nbytes < 2 * L2_BYTES
+              else f"arrays ({nbytes >> 20} MiB input) larger than L2 (126 MB); no flush",
     }
     if measure_e2e:
         res["e2e"] = run_e2e(x, lay, eb, mode, dim, steps, warmup, S)
@@ -557,7 +573,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": res["dtype"], "data": "synthetic (seeded)",
         "config": {"workload": args.workload, "desc": res["desc"], "n": res["n"], "dims": res["dims"],
                    "mode": res["mode"], "dim": res["dim"], "eb": res["eb"], "step": "compress + decompress",
-                   "l2": "inputs (512 MiB) larger than L2 (126 MB); no flush needed",
+                   "l2": res["l2"],
                    "parallelism": f"replicas x{world}"},
         "compress": rl["compress"], "decompress": rl["decompress"],
         "roofline": {k: rl[dominant][k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic")},
@@ -569,19 +585,12 @@ def main():
     }
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args.workload, device)
+    also = {}
     if not args.no_also:
-        also = {}
         for name in ALSO:
             r = run_workload(name, max(5, args.steps // 2), args.warmup, device, stream, 0, measure_e2e=False)
-            rr = roofline(r, peak, kind)
-            also[name] = {"compress_gbs": rr["compress"]["gbs_input"], "decompress_gbs": rr["decompress"]["gbs_input"],
-                          "compress_frac": rr["compress"]["frac"], "decompress_frac": rr["decompress"]["frac"],
-                          "compress_frac_of_8000": rr["compress"]["frac_of_8000"],
-                          "decompress_frac_of_8000": rr["decompress"]["frac_of_8000"],
-                          "compress_ms": r["compress_ms"], "decompress_ms": r["decompress_ms"], "cr": r["cr"],
-                          "over_1.1eb": r["over_1.1eb"], "launches": r["launches"]}
+            also[name] = (r, roofline(r, peak, kind))
             line["gpu_launches"] += r["launches"]
-        line["also"] = also
     if not args.no_forms and world == 1:
         try:
             line["batched"] = run_batched(device)
@@ -592,14 +601,33 @@ def main():
             line["serving"] = run_serving(device)
         except Exception as e:
             line["serving"] = {"error": f"{type(e).__name__}: {e}"}
+    # Compact per-workload figures last, so that the end of the line carries them:
+    # [compress GB/s of input, decompress GB/s, compress frac, decompress frac] (fractions
+    # of the measured HBM peak), kernel ms, ratio, FP64 check, L2 handling.
+    summ = {args.workload: _summary(res, rl)}
+    for name, (r, rr) in also.items():
+        summ[name] = _summary(r, rr)
+    line["summary"] = {"peak_gbs": peak, "peak_kind": kind, "frac_unit": "of measured" if kind == "measured"
+                       else "of fallback", "workloads": summ}
     print(json.dumps(line), flush=True)
+
+
+def _summary(r, rr):
+    c, d = rr["compress"], rr["decompress"]
+    return {"gbs": [round(c["gbs_input"], 1), round(d["gbs_input"], 1)],
+            "frac": [round(c["frac"], 4), round(d["frac"], 4)],
+            "frac_of_8000": [round(c["frac_of_8000"], 4), round(d["frac_of_8000"], 4)],
+            "ms": [round(r["compress_ms"], 4), round(r["decompress_ms"], 4)], "cr": round(r["cr"], 3),
+            "over_eb": r["over_eb"], "over_1.1eb": r["over_1.1eb"], "l2_flush": r["l2"].startswith("L2 flushed")}
 
 
 # ---------------------------------------------------------------------------- reference arm
 
 def reference_arm(args):
     """CPU oracle on the host cores (the reference has no CPU path), plus the
-    reference's CUDA build (sm_100) timed on the same GPU through its C API."""
+    reference's CUDA build (sm_100) on the same GPU: per call through its C API and
+    kernel-only, and a byte-for-byte comparison of its streams and reconstructions
+    with this library's on every single-array workload."""
     import torch
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
@@ -616,7 +644,128 @@ def reference_arm(args):
         line["reference_cuda_build"] = reference_cuda(args.workload, args.steps, args.warmup, device)
     except Exception as e:  # the CPU arm above is the reference arm; the GPU build is extra
         line["reference_cuda_build"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    if not args.no_also:
+        par = {}
+        for name in [args.workload] + [w for w in ALSO if w != args.workload]:
+            try:
+                par[name] = reference_parity(name, device)
+            except Exception as e:
+                par[name] = {"unavailable": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+        line["parity_vs_reference_build"] = par
     print(json.dumps(line), flush=True)
+
+
+def _ref_lib():
+    """The reference library compiled for sm_100 from its own sources (oracle/_ref),
+    with the ctypes signatures of its C entry points (include/cuSZp.h:38-45)."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libcuszp_ref.so")
+    if not os.path.exists(path):
+        raise FileNotFoundError("oracle/_ref/libcuszp_ref.so not built")
+    lib = ctypes.CDLL(path)
+    from cuszp_b200.pycuSZp import Uint3
+    lib.cuSZp_compress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                   ctypes.POINTER(ctypes.c_size_t), ctypes.c_float, ctypes.c_int, Uint3,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.cuSZp_decompress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
+                                     ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    return lib
+
+
+def _ref_kernel_lib():
+    """Kernel-only timing harness around the reference's kernels (oracle/ref_kernels.cu)."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libcuszp_refk.so")
+    if not os.path.exists(path):
+        raise FileNotFoundError("oracle/_ref/libcuszp_refk.so not built")
+    lib = ctypes.CDLL(path)
+    from cuszp_b200.pycuSZp import Uint3
+    lib.cuszp_refk_time.restype = ctypes.c_int
+    lib.cuszp_refk_time.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_size_t, Uint3, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_void_p]
+    return lib
+
+
+def reference_kernel_times(x, stream_buf, out, lay, eb, mode, reps=10, warmup=3):
+    """Kernel-only times (ms, mean of `reps`) of the reference's compress and decompress
+    kernels on device buffers: scratch zeroed outside the timed region, CUDA events
+    around the launch alone."""
+    import torch
+    from cuszp_b200 import codec
+    from cuszp_b200.pycuSZp import Uint3
+    lib = _ref_kernel_lib()
+    t, m = codec.TYPES[x.dtype], codec.MODES[mode]
+    ebk = float(ctypes.c_float(eb).value)   # the generic API's f64 path widens the float bound
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    res = {}
+    for d, (name, ptr) in enumerate((("compress", x), ("decompress", out))):
+        mean, best = ctypes.c_float(0), ctypes.c_float(0)
+        pay = ctypes.c_ulonglong(0)
+        rc = lib.cuszp_refk_time(d, t, lay.dim, m, ctypes.c_void_p(ptr.data_ptr()),
+                                 ctypes.c_void_p(stream_buf.data_ptr()), lay.n, Uint3(*lay.dims), ebk, warmup, reps,
+                                 ctypes.byref(mean), ctypes.byref(best), ctypes.byref(pay), s)
+        if rc != 0:
+            raise RuntimeError(f"reference kernel harness returned CUDA error {rc}")
+        res[name] = mean.value
+    torch.cuda.synchronize()
+    return res
+
+
+def reference_parity(name, device):
+    """Runs one workload through the reference build's stock C API and through this
+    library on the same device input, and compares the stream bytes [0, S) and the
+    reconstructions byte for byte (both output buffers pre-zeroed: the reference
+    leaves 2D/3D rate-region padding bytes and zero-rate blocks unwritten).  Also the
+    FP64 check of each reconstruction against eb and the reference's kernel-only times."""
+    import torch
+    from cuszp_b200 import codec
+    from cuszp_b200.pycuSZp import Uint3
+    lib = _ref_lib()
+    desc, dt, mode, dim, shape, ebk, ebv, gen = WORKLOADS[name]
+    x = make_input(name, device)
+    lay = codec.Layout.of(x, dim)
+    eb = codec.rel_error_bound(x, ebv) if ebk == "rel" else ebv
+    cap = codec.max_compressed_size(lay, x.dtype, mode)
+    t, m = codec.TYPES[x.dtype], codec.MODES[mode]
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc_ = torch.zeros(cap, dtype=torch.uint8, device=device)
+    ro = torch.zeros_like(x)
+    cs = ctypes.c_size_t(0)
+    lib.cuSZp_compress(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(rc_.data_ptr()), lay.n, ctypes.byref(cs),
+                       ctypes.c_float(eb), dim, Uint3(*lay.dims), t, m, s)
+    torch.cuda.synchronize()
+    ours = codec.compress(x, eb, mode, dim=dim, dims=lay.dims)
+    S = ours.numel()
+    lib.cuSZp_decompress(ctypes.c_void_p(ro.data_ptr()), ctypes.c_void_p(rc_.data_ptr()), lay.n, cs.value,
+                         ctypes.c_float(eb), dim, Uint3(*lay.dims), t, m, s)
+    torch.cuda.synchronize()
+    oo = codec.decompress(ours, x.shape, x.dtype, eb, mode, dim=dim, dims=lay.dims)
+    torch.cuda.synchronize()
+    stream_equal = bool(torch.equal(rc_[:S], ours))
+    recon_equal = bool(torch.equal(ro.reshape(-1).view(torch.uint8), oo.reshape(-1).view(torch.uint8)))
+    ebd = float(ctypes.c_float(eb).value)
+
+    def over(y):
+        err = (x.double() - y.double()).abs()
+        return int((err > ebd).sum().item()), int((err > 1.1 * ebd).sum().item())
+
+    ref_over = over(ro)
+    our_over = ref_over if recon_equal else over(oo)
+    out = {"S": S, "ref_cmpSize": cs.value, "stream_equal": stream_equal, "recon_equal": recon_equal,
+           "over_eb_ref": ref_over[0], "over_eb_ours": our_over[0], "over_1.1eb_ref": ref_over[1],
+           "over_1.1eb_ours": our_over[1]}
+    del ours, oo
+    try:
+        k = reference_kernel_times(x, rc_, ro, lay, eb, mode)
+        nb = x.numel() * x.element_size()
+        out["ref_kernel_ms"] = [round(k["compress"], 4), round(k["decompress"], 4)]
+        out["ref_kernel_gbs"] = [round(nb / (k["compress"] / 1e3) / 1e9, 1),
+                                 round(nb / (k["decompress"] / 1e3) / 1e9, 1)]
+    except Exception as e:
+        out["ref_kernel_ms"] = f"unavailable: {type(e).__name__}: {e}"
+    del x, rc_, ro
+    return out
 
 
 def reference_cuda(name, steps, warmup, device):
@@ -626,16 +775,8 @@ def reference_cuda(name, steps, warmup, device):
     blocking size read-back, as its CLI's timing does)."""
     import torch
     from cuszp_b200 import codec
-    path = os.path.join(ROOT, "oracle", "_ref", "libcuszp_ref.so")
-    if not os.path.exists(path):
-        return {"unavailable": "oracle/_ref/libcuszp_ref.so not built"}
-    lib = ctypes.CDLL(path)
     from cuszp_b200.pycuSZp import Uint3
-    lib.cuSZp_compress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
-                                   ctypes.POINTER(ctypes.c_size_t), ctypes.c_float, ctypes.c_int, Uint3,
-                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
-    lib.cuSZp_decompress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
-                                     ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib = _ref_lib()
     desc, dt, mode, dim, shape, ebk, ebv, gen = WORKLOADS[name]
     x = make_input(name, device)
     lay = codec.Layout.of(x, dim)
@@ -675,7 +816,8 @@ def reference_cuda(name, steps, warmup, device):
     c, d = statistics.mean(cms), statistics.mean(dms)
     return {"compress_gbs": nb / (c / 1e3) / 1e9, "decompress_gbs": nb / (d / 1e3) / 1e9,
             "round_trip_gbs": nb / ((c + d) / 1e3) / 1e9, "compress_ms": c, "decompress_ms": d,
-            "reported_cmpSize": cs.value, "build": "reference sources, nvcc -O3 sm_100 (oracle/Makefile ref)"}
+            "reported_cmpSize": cs.value, "timing": "per call, CUDA events (includes its scratch malloc/free)",
+            "build": "reference sources, nvcc -O3 sm_100 (oracle/Makefile ref)"}
 
 
 if __name__ == "__main__":

@@ -37,7 +37,7 @@ lib.cuSZp_max_compressed_size.argtypes = [_sz, ctypes.c_int, Uint3, ctypes.c_int
 lib.cuSZp_max_compressed_size.restype = _sz
 lib.cuSZp_workspace_size.argtypes = [_sz, ctypes.c_int, Uint3, ctypes.c_int, ctypes.c_int]
 lib.cuSZp_workspace_size.restype = _sz
-lib.cuSZp_compress_async.argtypes = [_vp, _vp, _sz, ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int,
+lib.cuSZp_compress_async.argtypes = [_vp, _vp, _sz, _sz, ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int,
                                      ctypes.c_int, _vp, _sz, _vp, _vp]
 lib.cuSZp_compress_async.restype = ctypes.c_int
 lib.cuSZp_decompress_async.argtypes = [_vp, _vp, _sz, ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int,
@@ -45,7 +45,7 @@ lib.cuSZp_decompress_async.argtypes = [_vp, _vp, _sz, ctypes.c_float, ctypes.c_i
 lib.cuSZp_decompress_async.restype = ctypes.c_int
 lib.cuSZp_workspace_check.argtypes = [_vp, _sz, _vp]
 lib.cuSZp_workspace_check.restype = ctypes.c_int
-lib.cuSZp_compress_ex.argtypes = [_vp, _vp, _sz, ctypes.POINTER(_sz), ctypes.c_float, ctypes.c_int, Uint3,
+lib.cuSZp_compress_ex.argtypes = [_vp, _vp, _sz, _sz, ctypes.POINTER(_sz), ctypes.c_float, ctypes.c_int, Uint3,
                                   ctypes.c_int, ctypes.c_int, _vp]
 lib.cuSZp_compress_ex.restype = ctypes.c_int
 lib.cuSZp_decompress_ex.argtypes = [_vp, _vp, _sz, _sz, ctypes.c_float, ctypes.c_int, Uint3, ctypes.c_int,
@@ -156,7 +156,8 @@ def compress_into(x: torch.Tensor, out: torch.Tensor, eb: float, mode="plain", d
     ws = workspace or default_workspace(x.device, stream)
     wsb = workspace_size(lay, x.dtype, mode)
     ws.ensure(wsb)
-    st = lib.cuSZp_compress_async(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), lay.n,
+    st = lib.cuSZp_compress_async(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                  out.numel() * out.element_size(), lay.n,
                                   ctypes.c_float(eb), lay.dim, Uint3(*lay.dims), TYPES[x.dtype], _mode(mode),
                                   ctypes.c_void_p(ws.ptr), ws.buf.numel(),
                                   ctypes.c_void_p(size_out.data_ptr()) if size_out is not None else None,

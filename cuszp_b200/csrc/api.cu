@@ -53,10 +53,21 @@ int check_ptrs(const Problem& p, const void* data, const void* cmp)
     return OK;
 }
 
+// Status of a launch's error word: a timed-out wait, else a stream that did not fit
+// its buffer (or, decompressing, rate bytes no valid stream holds).
+int status_of(uint32_t err)
+{
+    if (err & kTimeoutErrs) return E_TIMEOUT;
+    if (err & ERR_CAPACITY) return E_CAPACITY;
+    return OK;
+}
+
 // Synchronous call with a pool-allocated workspace.  Returns a Status; for
-// compress, *S receives the stream length.
+// compress, *S receives the stream length (also when the stream did not fit
+// `capacity`, E_CAPACITY: then it is the capacity needed).
 int run_sync(bool comp, const void* data_in, void* data_out, const uint8_t* cmp_in, uint8_t* cmp_out,
-             size_t nbEle, double eb, int dim, uint3 dims, int type, int mode, cudaStream_t stream, size_t* S)
+             size_t nbEle, double eb, int dim, uint3 dims, int type, int mode, cudaStream_t stream, size_t* S,
+             size_t capacity = ~(size_t)0)
 {
     Problem p;
     int st = make_problem(p, type, mode, dim, nbEle, dims.x, dims.y, dims.z);
@@ -64,6 +75,10 @@ int run_sync(bool comp, const void* data_in, void* data_out, const uint8_t* cmp_
     st = comp ? check_ptrs(p, data_in, cmp_out) : check_ptrs(p, data_out, cmp_in);
     if (st) return st;
     if (p.g.ntiles == 0) { if (S) *S = (size_t)p.g.rate_bytes; return OK; }
+    if (comp) {
+        if (capacity < p.g.rate_bytes) return E_CAPACITY;   // the rate region alone does not fit
+        p.g.cap = capacity;
+    }
     keep_pool_warm();
     const size_t wsb = workspace_bytes(p);
     void* ws = nullptr;
@@ -78,14 +93,14 @@ int run_sync(bool comp, const void* data_in, void* data_out, const uint8_t* cmp_
     const cudaError_t e = cudaStreamSynchronize(stream);
     if (st) return st;
     if (e != cudaSuccess) return E_CUDA;
-    if (h.err) return E_TIMEOUT;
-    if (S) *S = (size_t)h.total;
-    return OK;
+    st = status_of(h.err);
+    if (S && (st == OK || st == E_CAPACITY)) *S = (size_t)h.total;
+    return st;
 }
 
 void report(const char* what, int st)
 {
-    if (st == E_ARG || st == E_UNSUPPORTED || st == E_CUDA || st == E_TIMEOUT)
+    if (st == E_ARG || st == E_UNSUPPORTED || st == E_CUDA || st == E_TIMEOUT || st == E_CAPACITY)
         std::fprintf(stderr, "cuSZp: %s failed: %s\n", what, status_text(st));
 }
 
@@ -154,10 +169,10 @@ extern "C" size_t cuSZp_workspace_size(size_t nbEle, cuszp_dim_t dim, uint3 dims
     return workspace_bytes(p);
 }
 
-extern "C" int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
-                                    float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
-                                    cuszp_mode_t mode, void* d_workspace, size_t workspaceBytes,
-                                    unsigned long long* d_cmpSize, cudaStream_t stream)
+extern "C" int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpBytes, size_t cmpCapacity,
+                                    size_t nbEle, float errorBound, cuszp_dim_t dim, uint3 dims,
+                                    cuszp_type_t type, cuszp_mode_t mode, void* d_workspace,
+                                    size_t workspaceBytes, unsigned long long* d_cmpSize, cudaStream_t stream)
 {
     Problem p;
     int st = make_problem(p, type, mode, dim, nbEle, dims.x, dims.y, dims.z);
@@ -165,11 +180,12 @@ extern "C" int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpB
     if ((st = check_ptrs(p, d_oriData, d_cmpBytes))) return st;
     if (p.g.ntiles == 0) {
         if (d_cmpSize) {
-            static const unsigned long long zero = 0;
-            if (cudaMemcpyAsync(d_cmpSize, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream) != cudaSuccess) return E_CUDA;
+            if (cudaMemsetAsync(d_cmpSize, 0, sizeof(unsigned long long), stream) != cudaSuccess) return E_CUDA;
         }
         return OK;
     }
+    if (cmpCapacity < p.g.rate_bytes) return E_CAPACITY;   // the rate region alone does not fit
+    p.g.cap = cmpCapacity;
     if (!d_workspace || workspaceBytes < workspace_bytes(p) || (uintptr_t)d_workspace % 16) return E_WORKSPACE;
     if ((st = launch_compress(p, d_oriData, d_cmpBytes, (double)errorBound, d_workspace, stream))) return st;
     if (d_cmpSize) {
@@ -200,23 +216,27 @@ extern "C" int cuSZp_workspace_check(void* d_workspace, size_t workspaceBytes, c
     WsHeader h;
     if (cudaMemcpyAsync(&h, d_workspace, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return E_CUDA;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return E_CUDA;
-    if (h.err) {
+    const int st = status_of(h.err);
+    if (st == E_TIMEOUT) {
         // an aborted call may leave tickets and tile status behind: start clean
-        cudaMemsetAsync(d_workspace, 0, workspaceBytes, stream);
-        cudaStreamSynchronize(stream);
-        return E_TIMEOUT;
+        if (cudaMemsetAsync(d_workspace, 0, workspaceBytes, stream) != cudaSuccess) return E_CUDA;
+    } else if (st == E_CAPACITY) {
+        // the launch completed (the workspace is clean again): clear the error word only
+        if (cudaMemsetAsync(&reinterpret_cast<WsHeader*>(d_workspace)->err, 0, sizeof(uint32_t), stream) != cudaSuccess)
+            return E_CUDA;
     }
-    return OK;
+    if (st && cudaStreamSynchronize(stream) != cudaSuccess) return E_CUDA;
+    return st;
 }
 
-extern "C" int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle, size_t* cmpSize,
-                                 float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
-                                 cuszp_mode_t mode, cudaStream_t stream)
+extern "C" int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t cmpCapacity,
+                                 size_t nbEle, size_t* cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
+                                 cuszp_type_t type, cuszp_mode_t mode, cudaStream_t stream)
 {
     size_t S = 0;
     const int st = run_sync(true, d_oriData, nullptr, nullptr, d_cmpBytes, nbEle, (double)errorBound, dim, dims,
-                            type, mode, stream, &S);
-    if (cmpSize) *cmpSize = st ? 0 : S;
+                            type, mode, stream, &S, cmpCapacity);
+    if (cmpSize) *cmpSize = (st == OK || st == E_CAPACITY) ? S : 0;
     return st;
 }
 

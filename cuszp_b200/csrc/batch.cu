@@ -307,24 +307,19 @@ static const void* kernel_for_variant(int type, bool comp)
     return comp ? (const void*)compress_batch_kernel<double, DIM, Tl> : (const void*)decompress_batch_kernel<double, DIM, Tl>;
 }
 
-// Enables (once per device) the dynamic shared memory a kernel needs and returns it.
-static size_t enable_smem(const void* fn, size_t bytes, bool* set)
+// Enables (once per device) the dynamic shared memory a kernel needs and returns it
+// (a refusal surfaces as the launch's error).
+static size_t enable_smem(const void* fn, size_t bytes)
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !set[dev]) {
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        set[dev] = true;
-    }
+    enable_dynamic_smem(fn, bytes);
     return bytes;
 }
 
 template <typename T, int DIM, typename Tl>
 static size_t smem_for_variant(bool comp)
 {
-    static bool set[64] = {};   // the attribute is per device
     if (!comp) return 0;
-    return enable_smem((const void*)compress_batch_kernel<T, DIM, Tl>, compress_smem_bytes<T, DIM, Tl>(), set);
+    return enable_smem((const void*)compress_batch_kernel<T, DIM, Tl>, compress_smem_bytes<T, DIM, Tl>());
 }
 
 template <int WARPS, int BPW1D, int BPWND>
@@ -357,9 +352,8 @@ static const void* tma_batch_kernel(bool comp)
 template <typename T, int DIM>
 static size_t tma_batch_smem(bool comp)
 {
-    static bool set[2][64] = {};
-    return comp ? enable_smem(tma_batch_kernel<T, DIM>(true), TmaCfg<T, DIM>::smem_bytes(), set[0])
-                : enable_smem(tma_batch_kernel<T, DIM>(false), DecCfg<T, DIM>::smem_bytes(), set[1]);
+    return comp ? enable_smem(tma_batch_kernel<T, DIM>(true), TmaCfg<T, DIM>::smem_bytes())
+                : enable_smem(tma_batch_kernel<T, DIM>(false), DecCfg<T, DIM>::smem_bytes());
 }
 
 template <int N>
@@ -535,10 +529,8 @@ static int plan_launch(cuszp_batch_plan* p, unsigned long long* d_sizes, cudaStr
     const Variant& v = kVariants[p->variant];
     const void* fn = v.kernel(p->type, p->dim, p->compress);
     const size_t smem = v.smem(p->type, p->dim, p->compress);
-    int occ = 0;
     const int threads = v.threads(p->type, p->dim, p->compress);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem);
-    if (occ < 1) occ = 1;
+    const int occ = std::max(1, resident_ctas(fn, threads, smem));
     const int per_sm = p->ctas_per_sm > 0 ? std::min(p->ctas_per_sm, occ) : occ;
     const uint64_t want = (uint64_t)p->sms * per_sm;
     const unsigned grid = (unsigned)std::min<uint64_t>(want, p->total_tiles);
@@ -652,10 +644,8 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
         int st = plan_layout(p, v, stream);
         if (st) return st;
         const void* fn = kVariants[v].kernel(p->type, p->dim, p->compress);
-        int occ = 0;
         const size_t smem = kVariants[v].smem(p->type, p->dim, p->compress);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kVariants[v].threads(p->type, p->dim, p->compress),
-                                                      smem);
+        const int occ = resident_ctas(fn, kVariants[v].threads(p->type, p->dim, p->compress), smem);
         for (int c = 1; c <= std::max(1, occ); c++) {
             p->ctas_per_sm = c;
             plan_launch(p, d_sizes, stream);   // warm

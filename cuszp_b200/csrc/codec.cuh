@@ -15,6 +15,7 @@
 // Payload offsets come from a single-pass decoupled look-back over tiles.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -26,8 +27,12 @@ constexpr int kThreads = kWarps * 32;
 
 enum Mode : int { MODE_FIXED = 0, MODE_PLAIN = 1, MODE_OUTLIER = 2 };
 
-// Error bits reported through the workspace error word.
-enum : uint32_t { ERR_LOOKBACK_TIMEOUT = 1u, ERR_CAPACITY = 2u };
+// Error bits reported through the workspace error word.  The two timeout bits make
+// every other bounded wait of the launch give up as well; ERR_CAPACITY (a stream that
+// does not fit the caller's buffer, or rate bytes no valid stream holds) does not stop
+// the launch: its other tiles complete normally.
+enum : uint32_t { ERR_LOOKBACK_TIMEOUT = 1u, ERR_CAPACITY = 2u, ERR_WAIT_TIMEOUT = 4u };
+constexpr uint32_t kTimeoutErrs = ERR_LOOKBACK_TIMEOUT | ERR_WAIT_TIMEOUT;
 
 // Tile status word: [63:62] = 0 none / 1 aggregate / 2 inclusive prefix, [61:0] value.
 constexpr uint64_t ST_AGG = 1ull << 62;
@@ -42,11 +47,27 @@ struct WsHeader {
     uint32_t ticket;     // next tile to hand out
     uint32_t done;       // CTAs that finished (last one resets the workspace)
     uint32_t err;        // sticky error bits, read and cleared by the host
-    uint32_t pad;
-    unsigned long long total;   // true stream length S of the last call
+    uint32_t wait_cap;   // 0: default wait limits; else every bounded wait gives up after
+                         // this many polls (look-back) or sleep slices (mbarrier waits)
+    unsigned long long total;   // true stream length S of the last call (~0 after a timeout)
     unsigned long long pad2[3];
 };
 static_assert(sizeof(WsHeader) == 48, "header layout");
+static_assert(offsetof(WsHeader, wait_cap) == offsetof(WsHeader, err) + 4, "wait_cap follows err");
+
+// A wait's limit: the workspace's wait_cap when set (read through the error word's
+// address: the cap is the header word after it), else the default.  Waits read it only
+// once a first attempt has failed, so a wait that is already satisfied costs no load.
+__device__ __forceinline__ int wait_limit(const uint32_t* err, int dflt)
+{
+    const uint32_t cap = *reinterpret_cast<const volatile uint32_t*>(err + 1);
+    return cap ? (int)min(cap, 0x7fffffffu) : dflt;
+}
+// Whether a bounded wait elsewhere in the launch has given up.
+__device__ __forceinline__ bool timed_out(const uint32_t* err)
+{
+    return (*reinterpret_cast<const volatile uint32_t*>(err) & kTimeoutErrs) != 0;
+}
 
 // Unsigned 32-bit division by an invariant divisor d >= 1 as a multiply-high and shifts
 // (Granlund & Montgomery, "Division by invariant integers using multiplication",
@@ -82,6 +103,9 @@ struct Geom {
     FastDiv div_bx;        // division by bxn
     FastDiv div_plane;     // division by bxn * byn
     uint32_t grouped;      // TMA kernels, 2D: the tensor map's box is kGroup whole blocks
+    uint64_t cap;          // compress: bytes the stream buffer holds (~0: not checked); a
+                           // payload span that would end past it is not written and
+                           // ERR_CAPACITY is raised (the stream length is still computed)
 };
 
 // Blocks per tensor-map box of the TMA kernels' grouped 2D maps (one codec warp's share
@@ -349,6 +373,7 @@ __device__ __forceinline__ uint64_t warp_lookback(unsigned long long* status, in
 {
     const int lane = threadIdx.x & 31;
     constexpr long long NONE = -(1ll << 62);
+    int limit = 0;   // read at the first poll that finds a predecessor pending
     uint64_t excl = 0;
     int64_t hi = tile - 1;
     while (hi >= 0) {
@@ -378,7 +403,8 @@ __device__ __forceinline__ uint64_t warp_lookback(unsigned long long* status, in
                 pend_any |= (w[k] >> 62) == 0 && (long long)idx > jmax;
             }
             if (!__any_sync(FULL, pend_any)) break;
-            if (++spins > kSpinLimit) {
+            if (limit == 0) limit = wait_limit(err, kSpinLimit);
+            if (++spins > limit) {
                 if (lane == 0) atomicOr(err, ERR_LOOKBACK_TIMEOUT);
                 return excl;
             }
@@ -415,6 +441,8 @@ __device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* st
         if (threadIdx.x == 0) {
             hdr->ticket = 0u;
             hdr->done = 0u;
+            // a stream length after a timed-out wait may be partial: mark it invalid
+            if (timed_out(&hdr->err)) hdr->total = ~0ull;
         }
         __threadfence();
     }

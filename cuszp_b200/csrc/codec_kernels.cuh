@@ -700,6 +700,16 @@ __device__ __forceinline__ unsigned long long encode_tile(const T* __restrict__ 
     return agg;
 }
 
+// Writes a resolved tile's staged payload at its offset, unless it would end past the
+// stream buffer's capacity (then nothing is written and ERR_CAPACITY is raised).
+__device__ __forceinline__ void flush_tile(const uint8_t* __restrict__ sb, const TileCtx& c, unsigned long long agg,
+                                           unsigned long long base, uint32_t* err)
+{
+    const uint64_t at = c.g.rate_bytes + base;
+    if (at + agg <= c.g.cap) copy_out(sb, (uint32_t)agg, c.cmp + at);
+    else if (threadIdx.x == 0) atomicOr(err, ERR_CAPACITY);
+}
+
 // The tile loop shared by the single-array, batched and allocation-free kernels.
 // `Src` supplies tiles: take(sp, k) (thread 0: next ticket into slot k), ctx(sp, k, c)
 // (tile context of slot k; false once tiles run out), encode(...) (encode_tile with
@@ -734,7 +744,7 @@ __device__ __forceinline__ void compress_pipeline(Src& src, unsigned char* smem_
         const unsigned long long agg = src.encode(sm.in[b], ok0c, ok1c, cur, sm.sb[b], sp);
         if (has_prev) resolve_prev<Tl::WARPS>(prev, prev_agg, err, sp);
         __syncthreads();
-        if (has_prev) copy_out(sm.sb[prev_buf], (uint32_t)prev_agg, prev.cmp + prev.g.rate_bytes + sp.base);
+        if (has_prev) flush_tile(sm.sb[prev_buf], prev, prev_agg, sp.base, err);
         prev = cur;
         prev_agg = agg;
         prev_buf = b;
@@ -749,7 +759,7 @@ __device__ __forceinline__ void compress_pipeline(Src& src, unsigned char* smem_
     if (has_prev) {
         resolve_prev<Tl::WARPS>(prev, prev_agg, err, sp);
         __syncthreads();
-        copy_out(sm.sb[prev_buf], (uint32_t)prev_agg, prev.cmp + prev.g.rate_bytes + sp.base);
+        flush_tile(sm.sb[prev_buf], prev, prev_agg, sp.base, err);
     }
 }
 

@@ -8,7 +8,9 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 namespace cuszp {
 
@@ -21,6 +23,7 @@ int make_problem(Problem& p, int type, int mode, int dim, size_t nbEle, unsigned
     Geom& g = p.g;
     g.nbEle = nbEle;
     g.dx = dx; g.dy = dy; g.dz = dz;
+    g.cap = ~0ull;
     if (dim == 1) {
         g.nblocks = (nbEle + 31) / 32;
         g.rate_bytes = ((uint64_t)nbEle + 32767) / 32768 * 32768 / 32;
@@ -58,6 +61,64 @@ size_t max_stream_bytes(const Problem& p)
     return (size_t)(p.g.rate_bytes + p.g.nblocks * (W + 4 + 32 * W));
 }
 
+// ------------------------------------------------------------------ per-device set-up
+
+namespace {
+std::mutex g_setup_mu;
+struct SetupEnt {
+    const void* fn;
+    int dev;
+    int threads;
+    size_t smem;
+    int occ;   // -1: dynamic shared memory enabled (no occupancy entry)
+};
+std::vector<SetupEnt> g_setup;
+int g_sms[64] = {};
+}  // namespace
+
+bool enable_dynamic_smem(const void* fn, size_t bytes)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    for (const SetupEnt& e : g_setup)
+        if (e.fn == fn && e.dev == dev && e.occ < 0 && e.smem >= bytes) return true;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+        cudaGetLastError();   // not sticky: leave no error for the caller's next check
+        return false;
+    }
+    g_setup.push_back(SetupEnt{fn, dev, 0, bytes, -1});
+    return true;
+}
+
+int resident_ctas(const void* fn, int threads, size_t smem)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    for (const SetupEnt& e : g_setup)
+        if (e.fn == fn && e.dev == dev && e.occ >= 0 && e.threads == threads && e.smem == smem) return e.occ;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    g_setup.push_back(SetupEnt{fn, dev, threads, smem, occ});
+    return occ;
+}
+
+int sm_count()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 0;
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (dev < 64 && g_sms[dev]) return g_sms[dev];
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (dev < 64) g_sms[dev] = n;
+    return n;
+}
+
 // ------------------------------------------------------------------ dispatch tables
 
 struct KernelRef {
@@ -70,15 +131,9 @@ template <typename T, int DIM, int MODE>
 static KernelRef ckernel()
 {
     using Tl = Tiling<DIM>;
-    static bool set[64] = {};   // the attribute is per device
     const void* fn = (const void*)compress_kernel<T, DIM, MODE, Tl>;
     constexpr size_t bytes = compress_smem_bytes<T, DIM, Tl>();
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !set[dev]) {
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        set[dev] = true;
-    }
+    enable_dynamic_smem(fn, bytes);   // a refusal surfaces as the launch's error
     return {fn, bytes, kThreads};
 }
 template <typename T, int DIM, int MODE>
@@ -114,29 +169,12 @@ static KernelRef kernel_for(const Problem& p, bool comp)
 }
 
 // Persistent grid: every SM filled to the kernel's occupancy, never more CTAs than tiles.
-static int grid_for(const KernelRef& k, uint64_t ntiles)
+static unsigned grid_for(const KernelRef& k, uint64_t ntiles)
 {
-    static std::mutex mu;
-    static int sms[64] = {0};
-    struct Ent { const void* fn; int dev; int occ; };
-    static Ent cache[256];
-    static int ncache = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int occ = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (dev < 64 && sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
-        for (int i = 0; i < ncache; i++)
-            if (cache[i].fn == k.fn && cache[i].dev == dev) { occ = cache[i].occ; break; }
-        if (occ == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, k.smem);
-            if (occ < 1) occ = 1;
-            if (ncache < 256) cache[ncache++] = Ent{k.fn, dev, occ};
-        }
-    }
-    const uint64_t want = (uint64_t)(dev < 64 ? sms[dev] : 148) * (uint64_t)occ;
-    return (int)(ntiles < want ? ntiles : want);
+    const int occ = std::max(1, resident_ctas(k.fn, (int)k.threads, k.smem));
+    const int sms = sm_count();
+    const uint64_t want = (uint64_t)(sms > 0 ? sms : 148) * (uint64_t)occ;
+    return (unsigned)(ntiles < want ? ntiles : want);
 }
 
 // ------------------------------------------------------------------ TMA compress path
@@ -198,15 +236,9 @@ bool make_block_map(CUtensorMap* m, const Problem& p, const void* in, bool* grou
 template <typename T, int DIM, int MODE>
 static KernelRef tma_kernel()
 {
-    static bool set[64] = {};   // the attribute is per device
     const void* fn = (const void*)compress_tma_kernel<T, DIM, MODE>;
     constexpr size_t bytes = TmaCfg<T, DIM>::smem_bytes();
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !set[dev]) {
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        set[dev] = true;
-    }
+    enable_dynamic_smem(fn, bytes);
     return {fn, bytes, TmaCfg<T, DIM>::THREADS};
 }
 
@@ -252,25 +284,7 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
     bool grouped = false;
     if (p.dim != 1 && !make_block_map(&map, p, in, &grouped)) return -1;
     const KernelRef k = tma_kernel_for(p);
-    static std::mutex mu;
-    static int sms[64] = {0};
-    static int occ_cache[64][2][3][3] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return -1;
-    int occ = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
-        int& c = occ_cache[dev][p.type][p.dim - 1][p.mode];
-        if (c == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, k.threads, k.smem);
-            if (c < 1) c = 1;
-        }
-        occ = c;
-    }
-    const uint64_t want = (uint64_t)sms[dev] * (uint64_t)occ;
-    const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
+    const unsigned grid = grid_for(k, p.g.ntiles);
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
     Geom g = p.g;
@@ -287,15 +301,9 @@ static int launch_tma(const Problem& p, const void* in, void* cmp, double eb, vo
 template <typename T, int DIM, int MODE, bool DIRECT = false>
 static KernelRef dtma_kernel()
 {
-    static bool set[64] = {};   // the attribute is per device
     const void* fn = (const void*)decompress_tma_kernel<T, DIM, MODE, DIRECT>;
     constexpr size_t bytes = DecCfg<T, DIM, DIRECT>::smem_bytes();
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !set[dev]) {
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        set[dev] = true;
-    }
+    enable_dynamic_smem(fn, bytes);
     return {fn, bytes, DecCfg<T, DIM, DIRECT>::THREADS};
 }
 
@@ -344,26 +352,8 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     bool grouped = false;
     if (p.dim != 1 && !make_block_map(&map, p, out, &grouped)) return -1;
     const KernelRef k = dtma_kernel_for(p, grouped);
-    static std::mutex mu;
-    static int sms[64] = {0};
-    static int occ_cache[64][2][3][3][2] = {};   // [device][type][dim][mode][grouped]
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return -1;
     const unsigned threads = k.threads;
-    int occ = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (sms[dev] == 0) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
-        int& c = occ_cache[dev][p.type][p.dim - 1][p.mode][grouped ? 1 : 0];
-        if (c == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k.fn, threads, k.smem);
-            if (c < 1) c = 1;
-        }
-        occ = c;
-    }
-    const uint64_t want = (uint64_t)sms[dev] * (uint64_t)occ;
-    const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
+    const unsigned grid = grid_for(k, p.g.ntiles);
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
     Geom g = p.g;
@@ -389,7 +379,7 @@ static int launch(const Problem& p, bool comp, const void* a0, void* a1, double 
         if (st >= 0) return st;
     }
     const KernelRef k = kernel_for(p, comp);
-    const int grid = grid_for(k, p.g.ntiles);
+    const unsigned grid = grid_for(k, p.g.ntiles);
     WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
     unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader));
     Geom g = p.g;

@@ -55,6 +55,15 @@ int launch_decompress(const Problem& p, void* d_out, const uint8_t* d_cmp, doubl
 bool tma_allowed();
 bool make_block_map(CUtensorMap* m, const Problem& p, const void* data, bool* grouped);
 
+// Per-device kernel set-up shared by every launch path, thread-safe and cached per
+// (device, kernel): enable_dynamic_smem sets a kernel's dynamic shared-memory limit the
+// first time it is needed on the current device (false if the runtime refused; the next
+// call tries again); resident_ctas is the kernel's occupancy in CTAs per SM (0 if the
+// query failed); sm_count is the current device's SM count (0 on failure).
+bool enable_dynamic_smem(const void* fn, size_t bytes);
+int resident_ctas(const void* fn, int threads, size_t smem);
+int sm_count();
+
 // Value range (min, max) of a device array with the reference CLI's semantics
 // (examples/cuSZp.cpp:176-187): NaNs are skipped unless the first element is NaN.
 // Writes two values of the array's type to d_minmax; needs range_ws_bytes() of workspace.

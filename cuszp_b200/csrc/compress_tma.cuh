@@ -74,7 +74,6 @@ struct TmaCfg {
 
 constexpr int kWaitLimit = 1 << 18;       // bounded mbarrier waits: attempts of up to kWaitSliceNs each
 constexpr uint32_t kWaitSliceNs = 8192;  // (so a wait gives up after about two seconds)
-enum : uint32_t { ERR_WAIT_TIMEOUT = 4u };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -132,15 +131,27 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity)
     return ok != 0;
 }
 // Waits for the phase with `parity` to complete; false (and the error bit set) if it
-// did not within the limit.
+// did not within the limit, or at once false when another wait of the launch gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint32_t* err)
 {
-    for (int i = 0; i < kWaitLimit; i++) {
+    if (mbar_try_wait_ns(b, parity, kWaitSliceNs)) return true;
+    const int limit = wait_limit(err, kWaitLimit);
+    for (int i = 1; i < limit; i++) {
+        if (timed_out(err)) return false;   // another wait gave up
         if (mbar_try_wait_ns(b, parity, kWaitSliceNs)) return true;
-        if (*reinterpret_cast<volatile uint32_t*>(err)) return false;   // another wait gave up
     }
     atomicOr(err, ERR_WAIT_TIMEOUT);
     return false;
+}
+// Waits for the completion of a bulk copy already issued into this CTA's shared memory
+// (the phase with `parity` of its barrier), whatever else gave up: a CTA must not end
+// while a copy still writes its shared memory.  Bounded by the default limit (a copy
+// from the GPU's own memory completes in microseconds).
+__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity, uint32_t* err)
+{
+    for (int i = 0; i < kWaitLimit; i++)
+        if (mbar_try_wait_ns(b, parity, kWaitSliceNs)) return;
+    atomicOr(err, ERR_WAIT_TIMEOUT);
 }
 
 // One tensor box (coordinates x fastest) into shared memory, completing on `bar`.
@@ -492,10 +503,12 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
             const int c = k % C::NC;
             const uint32_t parity = (uint32_t)(k / C::NC) & 1u;
             bool ready = false;
-            for (int i = 0; i < 4 * kWaitLimit; i++) {   // tile k coded and its size posted, or no tile k
+            int limit = 1;   // read once a first attempt failed
+            for (int i = 0; i < limit; i++) {   // tile k coded and its size posted, or no tile k
                 if (mbar_try_wait_ns(&sh.aggd[c], parity, kWaitSliceNs / 4)) { ready = true; break; }
                 if (k >= *reinterpret_cast<volatile int*>(&sh.kend)) break;
-                if (*reinterpret_cast<volatile uint32_t*>(err)) break;
+                if (timed_out(err)) break;
+                if (i == 0) limit = 4 * min(wait_limit(err, kWaitLimit), kWaitLimit);
             }
             if (!ready) break;
             const TileArray A = src.array(sh.arr_of[c]);
@@ -593,7 +606,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
         if (lane == 0) {
             for (int s = 0; s < C::NIN; s++) {
                 const int uses = issued / C::NIN + (s < issued % C::NIN ? 1 : 0);
-                if (uses) mbar_wait(&sh.full[s], (uint32_t)(uses - 1) & 1u, err);
+                if (uses) mbar_drain(&sh.full[s], (uint32_t)(uses - 1) & 1u, err);
             }
         }
         __syncwarp();
@@ -626,7 +639,9 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
             const bool done = mbar_wait(&sh.based[c], (uint32_t)(q0.k / C::NC) & 1u, err);
             if (done) {
                 const TileArray A = src.array(sh.arr_of[c]);
-                warp_copy_out(ring + q0.at, q0.n, A.cmp + A.g->rate_bytes + sh.base[c] + sh.woff[c][warp], lane);
+                const uint64_t at = A.g->rate_bytes + sh.base[c] + sh.woff[c][warp];
+                if (at + q0.n <= A.g->cap) warp_copy_out(ring + q0.at, q0.n, A.cmp + at, lane);
+                else if (lane == 0) atomicOr(err, ERR_CAPACITY);   // nothing written past the buffer
                 __syncwarp();
             }
 #pragma unroll

@@ -490,13 +490,14 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
         constexpr int LPW = C::BPW / PER; // lanes per codec warp
         const int G = min(src.ticket_tiles(), GM);
         int m = 0;                        // fills of the slot so far
+        bool failed = false;              // left after a wait gave up
         for (;;) {
             int64_t gi = 0;
             if (lane == 0) gi = (int64_t)atomicAdd(&hdr->ticket, 1u);
             gi = __shfl_sync(FULL, gi, 0);
             const int64_t t0 = gi * G;
             if ((uint64_t)t0 >= ntotal) {   // no more tiles: an empty fill ends the slot
-                if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) break;
+                if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) { failed = true; break; }
                 if (lane == 0) {
                     sh.tile[f] = t0;
                     mbar_arrive(&sh.full[f]);
@@ -575,8 +576,12 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
                 p0 = p1;
                 m++;
             }
-            if (stop) break;
+            if (stop) { failed = true; break; }
         }
+        // fill m - 1 may still be loading when a wait gave up: the CTA must not end
+        // before that copy into its shared memory has landed
+        if (failed && m > 0 && lane == 0) mbar_drain(&sh.full[f], (uint32_t)(m - 1) & 1u, err);
+        __syncwarp();
     } else {
         // ---------------------------------------------------------------- codec warps
         T* ob = obuf + warp * (C::BPW * C::BLK);

@@ -23,9 +23,11 @@
 
 namespace cuszp {
 
-// 1 MiB: a 48-byte header plus 131,066 tile-status words, i.e. arrays of up to
-// 536,805,376 elements in 1D (4,096 elements per tile) and the same number of
-// elements in 2D/3D (64 blocks of 64 elements per tile).
+// 1 MiB: a 48-byte header plus 131,066 tile-status words.  In 1D a tile is 128 blocks of
+// 32 elements and the tile count is rounded up to whole 1,024-block rate granules (8
+// tiles), so 1D arrays of up to 16,383 x 32,768 = 536,838,144 elements fit; in 2D/3D a
+// tile is 64 data blocks, so up to 8,388,224 blocks fit (536,846,336 elements when every
+// block is whole).
 constexpr size_t kNoAllocScratchBytes = 1u << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -82,25 +84,37 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
 int g_sms[kMaxDevices] = {};
+// per device and kernel (type x dim x mode): CTAs per SM, 0 until the kernel's shared
+// memory limit is set and its occupancy known
+int g_occ[kMaxDevices][2][3][3] = {};
 
 // Once per device, with that device current: the array's device address (in host
-// code the symbol itself is only a host-side stand-in) and the SM count.
-int device_setup(int dev, unsigned char** addr, int* sms)
+// code the symbol itself is only a host-side stand-in) and the SM count; once per device
+// and kernel: the kernel's shared-memory limit and occupancy.
+int device_setup(int dev, const Problem& p, const void* fn, size_t smem, unsigned char** addr, int* sms, int* occ)
 {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
+        void* a = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+        if (e != cudaSuccess || !a) {
             std::fprintf(stderr, "cuSZp_compress_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
                          cudaGetErrorString(e));
             return E_CUDA;
         }
         if (cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return E_CUDA;
-        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+        g_scratch_addr[dev] = static_cast<unsigned char*>(a);
+    }
+    int& o = g_occ[dev][p.type][p.dim - 1][p.mode];
+    if (o == 0) {
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return E_CUDA;
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, smem) != cudaSuccess) return E_CUDA;
+        o = n < 1 ? 1 : n;
     }
     *addr = g_scratch_addr[dev];
     *sms = g_sms[dev];
+    *occ = o;
     return OK;
 }
 
@@ -134,17 +148,13 @@ extern "C" int cuSZp_compress_noalloc(const void* d_oriData, unsigned char* d_cm
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return E_CUDA;
-    unsigned char* ws = nullptr;
-    int sms = 0;
-    if ((st = device_setup(dev, &ws, &sms))) return st;
-    // a previous call may have been aborted mid-way: start from zero
-    if (cudaMemsetAsync(ws, 0, need, stream) != cudaSuccess) return E_CUDA;
     size_t smem = 0;
     const void* fn = noalloc_kernel(p, &smem);
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return E_CUDA;
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, smem);
-    if (occ < 1) occ = 1;
+    unsigned char* ws = nullptr;
+    int sms = 0, occ = 0;
+    if ((st = device_setup(dev, p, fn, smem, &ws, &sms, &occ))) return st;
+    // a previous call may have been aborted mid-way: start from zero
+    if (cudaMemsetAsync(ws, 0, need, stream) != cudaSuccess) return E_CUDA;
     const uint64_t want = (uint64_t)sms * occ;
     const unsigned grid = (unsigned)(p.g.ntiles < want ? p.g.ntiles : want);
     Geom g = p.g;

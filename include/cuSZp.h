@@ -105,13 +105,18 @@ size_t cuSZp_max_compressed_size(size_t nbEle, cuszp_dim_t dim, uint3 dims,
 size_t cuSZp_workspace_size(size_t nbEle, cuszp_dim_t dim, uint3 dims,
                             cuszp_type_t type, cuszp_mode_t mode);
 
-/* Enqueue compression on `stream` without synchronizing.  The stream length S is
- * written to *d_cmpSize (a device uint64) when d_cmpSize is non-null.  Calls that
- * share a workspace must be ordered (same stream or explicit dependencies). */
-int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
-                         float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
-                         cuszp_mode_t mode, void* d_workspace, size_t workspaceBytes,
-                         unsigned long long* d_cmpSize, cudaStream_t stream);
+/* Enqueue compression on `stream` without synchronizing.  `cmpCapacity` is the size of
+ * d_cmpBytes in bytes: nothing is written past it (cuSZp_max_compressed_size() always
+ * suffices).  A stream that does not fit is reported by cuSZp_workspace_check() as
+ * CUSZP_ERROR_CAPACITY; *d_cmpSize then still receives the length S it needs.  A
+ * capacity below the rate region fails at once with CUSZP_ERROR_CAPACITY.  S is
+ * written to *d_cmpSize (a device uint64) when d_cmpSize is non-null (~0 if a device
+ * wait timed out).  Calls that share a workspace must be ordered (same stream or
+ * explicit dependencies). */
+int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpBytes, size_t cmpCapacity,
+                         size_t nbEle, float errorBound, cuszp_dim_t dim, uint3 dims,
+                         cuszp_type_t type, cuszp_mode_t mode, void* d_workspace,
+                         size_t workspaceBytes, unsigned long long* d_cmpSize, cudaStream_t stream);
 
 /* Enqueue decompression on `stream` without synchronizing. */
 int cuSZp_decompress_async(void* d_decData, const unsigned char* d_cmpBytes, size_t nbEle,
@@ -120,14 +125,20 @@ int cuSZp_decompress_async(void* d_decData, const unsigned char* d_cmpBytes, siz
                            cudaStream_t stream);
 
 /* Synchronize `stream`, then read and clear the workspace's error word:
- * CUSZP_SUCCESS, or CUSZP_ERROR_TIMEOUT if a device-side wait gave up (the
- * workspace is re-zeroed so it can be reused). */
+ * CUSZP_SUCCESS; CUSZP_ERROR_TIMEOUT if a device-side wait gave up (the workspace is
+ * re-zeroed so it can be reused); CUSZP_ERROR_CAPACITY if a compressed stream did not
+ * fit its buffer, or a decompressed stream held rate bytes no valid stream holds.
+ * Word 3 of a workspace (uint32 at byte offset 12, normally 0) caps every bounded
+ * device-side wait of the calls using it at that many polls / sleep slices instead
+ * of the default of about two seconds; tests use it to make a wait run out fast. */
 int cuSZp_workspace_check(void* d_workspace, size_t workspaceBytes, cudaStream_t stream);
 
 /* Synchronous forms with a status and the true stream length; workspace is taken
- * from the device's stream-ordered memory pool. */
-int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t nbEle,
-                      size_t* cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
+ * from the device's stream-ordered memory pool.  Compress writes nothing past
+ * `cmpCapacity` bytes of d_cmpBytes; when the stream does not fit it returns
+ * CUSZP_ERROR_CAPACITY and *cmpSize receives the capacity needed. */
+int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t cmpCapacity,
+                      size_t nbEle, size_t* cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
                       cuszp_type_t type, cuszp_mode_t mode, cudaStream_t stream);
 int cuSZp_decompress_ex(void* d_decData, const unsigned char* d_cmpBytes, size_t nbEle,
                         size_t cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
@@ -198,9 +209,11 @@ void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t plan, cudaStream_t stream
  * that cannot allocate device memory when they compress (allocation forbidden or too
  * slow where they run, or all memory owned by a host framework): the look-back scratch
  * is a fixed 1 MiB array inside this library on each device, so the call allocates
- * nothing and needs no workspace.  Limit: arrays of at most 131,066 tiles (536,805,376
- * elements; 4,096 elements per tile); larger arrays are rejected with
- * CUSZP_ERROR_WORKSPACE and a message on stderr.  Asynchronous on `stream`; the stream
+ * nothing and needs no workspace.  Limit: 131,066 tiles of look-back state, i.e. 1D
+ * arrays of at most 536,838,144 elements (tiles of 4,096 elements, counted in whole
+ * 32,768-element rate granules) and 2D/3D arrays of at most 8,388,224 data blocks
+ * (tiles of 64 blocks; 536,846,336 elements when every block is whole); larger arrays
+ * are rejected with CUSZP_ERROR_WORKSPACE and a message on stderr.  Asynchronous on `stream`; the stream
  * length goes to *d_cmpSize (device uint64, required), or ~0 if a bounded device-side
  * wait gave up.  The first call on a device looks up the array's device address; make
  * that first call before any stream capture.  All calls on a device share the array:

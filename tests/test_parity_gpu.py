@@ -238,11 +238,17 @@ def test_status_codes():
         codec.compress(x, 1e-3, "plain", dim=2, dims=(10, 10, 10))     # dims.x % 4 != 0
     assert e.value.status == 2
     out = torch.empty(16, dtype=torch.uint8, device="cuda")
-    st = codec.lib.cuSZp_compress_async(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), 1000,
-                                        ctypes.c_float(1e-3), 1, codec.Uint3(0, 0, 0), 0, 1, None, 0, None, None)
+    big = torch.empty(1 << 16, dtype=torch.uint8, device="cuda")
+    st = codec.lib.cuSZp_compress_async(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(big.data_ptr()), big.numel(),
+                                        1000, ctypes.c_float(1e-3), 1, codec.Uint3(0, 0, 0), 0, 1, None, 0, None,
+                                        None)
     assert st == 5   # workspace missing
-    st = codec.lib.cuSZp_compress_ex(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), 1000, None,
-                                     ctypes.c_float(1e-3), 1, codec.Uint3(0, 0, 0), 7, 1, None)
+    st = codec.lib.cuSZp_compress_async(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), out.numel(),
+                                        1000, ctypes.c_float(1e-3), 1, codec.Uint3(0, 0, 0), 0, 1, None, 0, None,
+                                        None)
+    assert st == 6   # 16 bytes cannot hold the 1024-byte rate region
+    st = codec.lib.cuSZp_compress_ex(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), out.numel(),
+                                     1000, None, ctypes.c_float(1e-3), 1, codec.Uint3(0, 0, 0), 7, 1, None)
     assert st == 1   # bad type
 
 
