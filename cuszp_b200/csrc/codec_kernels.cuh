@@ -381,6 +381,33 @@ __device__ __forceinline__ void pack_block_nd(uint32_t r, int32_t c0, int32_t c1
     }
 }
 
+// The transpose input word of two 16-bit element slots: magnitudes in bits 0-14 (a) and
+// 16-30 (b), signs in bits 15 and 31.  A magnitude with bits above 14 (a 1D |INT_MIN|
+// code, which the 1D rate ignores) must not reach the sign bits, hence the masks.
+__device__ __forceinline__ uint32_t slot_pair(int32_t a, int32_t b)
+{
+    return (uabs(a) & 0x7fffu) | ((uabs(b) << 16) & 0x7fff0000u) | (((uint32_t)a >> 16) & 0x8000u) |
+           ((uint32_t)b & 0x80000000u);
+}
+
+// Payloads of four 1D blocks of rate <= 15: the pairs (A, B) and (C, D) take one
+// transpose each, interleaved.  After the transposes lane l holds plane pl = (l ^ 7) & 15
+// of block A / C (l < 16) or B / D (l >= 16), plane 15 being the block's sign word; the
+// lane stores it at its block's sign-word offset p1 / p2 plus `o` (0 for the sign word,
+// 4 + 4 pl for a plane) when that bit of the block's plane mask k1 / k2 is set.  In
+// outlier mode element 0's magnitude must already be cleared (sign kept) in blocks that
+// store element 0 ahead of their planes.
+template <int MODE>
+__device__ __forceinline__ void pack_quad_1d_narrow(int32_t cA, int32_t cB, int32_t cC, int32_t cD, uint32_t k1,
+                                                    saddr_t p1, uint32_t k2, saddr_t p2, uint32_t pl, uint32_t o,
+                                                    const XposeLane& xl)
+{
+    uint32_t x1 = slot_pair(cA, cB), x2 = slot_pair(cC, cD);
+    warp_transpose32x2(x1, x2, xl);
+    if ((k1 >> pl) & 1u) put32s<MODE>(p1 + o, x1);
+    if ((k2 >> pl) & 1u) put32s<MODE>(p2 + o, x2);
+}
+
 // Payloads of two 2D/3D blocks of rate <= 15, sign words at pa / pb, transposes
 // interleaved.  Lane l holds plane (l ^ 7) & 15 of half l >> 4 after the transpose
 // (plane 15 = the half's signs) and stores it when that bit of the block's plane mask
@@ -391,11 +418,7 @@ template <int MODE>
 __device__ __forceinline__ void pack_pair_narrow(uint32_t ka, uint32_t kb, int32_t c0a, int32_t c1a, int32_t c0b,
                                                  int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
 {
-    const uint32_t a0a = uabs(c0a), a0b = uabs(c0b), a1a = uabs(c1a), a1b = uabs(c1b);
-    uint32_t xa = (a0a & 0x7fffu) | ((a1a << 16) & 0x7fff0000u) | (((uint32_t)c0a >> 16) & 0x8000u) |
-                  ((uint32_t)c1a & 0x80000000u);
-    uint32_t xb = (a0b & 0x7fffu) | ((a1b << 16) & 0x7fff0000u) | (((uint32_t)c0b >> 16) & 0x8000u) |
-                  ((uint32_t)c1b & 0x80000000u);
+    uint32_t xa = slot_pair(c0a, c1a), xb = slot_pair(c0b, c1b);
     warp_transpose32x2(xa, xb, xl);
     const uint32_t pl = (lane ^ 7) & 15;
     const uint32_t h4 = (uint32_t)(lane >> 4) * 4;

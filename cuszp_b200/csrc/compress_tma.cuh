@@ -249,6 +249,7 @@ __device__ __forceinline__ uint32_t codes_1d(saddr_t tin, WarpCodes<1, C>& K, in
         if (lane == j + 1) { M = mB; O = oB; }
     }
     K.rb = lane < C::BPW ? rate_byte<1, MODE>(M, O) : 0u;
+    K.o = O;
     if (lane < C::BPW && b0 + lane < g.rate_bytes) cmp[b0 + lane] = (uint8_t)K.rb;
     return __reduce_add_sync(FULL, payload_size<1, MODE>(K.rb));
 }
@@ -343,6 +344,50 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
         if (lane >= o) incl += v;
     }
     uint32_t myoff = incl - sz;
+    if constexpr (DIM == 1) {
+        const uint32_t n = MODE == MODE_OUTLIER ? (mine & 0x1fu) : mine;
+        if (__all_sync(FULL, n <= 15)) {
+            // every block narrow: four blocks per step, no branches between them; lane j
+            // holds block j's plane mask and sign-word offset
+            uint32_t ps = myoff, heads = 0;
+            if constexpr (MODE == MODE_OUTLIER) {
+                // element 0's bytes of every outlier block: lane 4j + i writes byte i of
+                // block j, eight blocks per step; the sign words follow them
+                const uint32_t ob = (mine & 0x80u) ? ((mine & 0x60u) >> 5) + 1u : 0u;
+                const uint32_t i = lane & 3;
+#pragma unroll
+                for (int h = 0; h < C::BPW; h += 8) {
+                    const int src = h + (lane >> 2);
+                    const uint32_t nb = __shfl_sync(FULL, ob, src), v = __shfl_sync(FULL, K.o, src);
+                    const uint32_t at = __shfl_sync(FULL, myoff, src);
+                    if (i < nb) sts_u8(out + at + i, v >> (8 * i));
+                }
+                heads = __ballot_sync(FULL, ob != 0);
+                ps += ob;
+            }
+            const uint32_t mask = plane_mask(mine, n);
+            const int half = lane >> 4;
+            const uint32_t pl = (uint32_t)(lane ^ 7) & 15u;
+            const uint32_t o = pl == 15 ? 0u : 4u + 4u * pl;
+#pragma unroll
+            for (int j = 0; j < C::BPW; j += 4) {
+                const uint32_t k1 = __shfl_sync(FULL, mask, j + half), k2 = __shfl_sync(FULL, mask, j + 2 + half);
+                const uint32_t p1 = __shfl_sync(FULL, ps, j + half), p2 = __shfl_sync(FULL, ps, j + 2 + half);
+                int32_t cA = K.c0[j], cB = K.c0[j + 1], cC = K.c0[j + 2], cD = K.c0[j + 3];
+                if constexpr (MODE == MODE_OUTLIER) {
+                    // magnitude 0 in the planes where element 0 went ahead of them, sign kept
+                    if (lane == 0) {
+                        if ((heads >> j) & 1u) cA = (int32_t)((uint32_t)cA & 0x80000000u);
+                        if ((heads >> (j + 1)) & 1u) cB = (int32_t)((uint32_t)cB & 0x80000000u);
+                        if ((heads >> (j + 2)) & 1u) cC = (int32_t)((uint32_t)cC & 0x80000000u);
+                        if ((heads >> (j + 3)) & 1u) cD = (int32_t)((uint32_t)cD & 0x80000000u);
+                    }
+                }
+                pack_quad_1d_narrow<MODE>(cA, cB, cC, cD, k1, out + p1, k2, out + p2, pl, o, xl);
+            }
+            return;
+        }
+    }
     if constexpr (DIM != 1) {
         if constexpr (MODE == MODE_OUTLIER) {
             // element 0's bytes of every outlier block at once: lane 4j + i writes byte i of

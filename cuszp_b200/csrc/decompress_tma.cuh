@@ -228,6 +228,39 @@ __device__ __forceinline__ void decode_pair_narrow(saddr_t pay, uint32_t pa, uin
     d1b = (xb & 0x80000000u) ? (int32_t)(0u - m1b) : (int32_t)m1b;
 }
 
+// Four 1D blocks with at most 15 planes each: the pairs (A, B) and (C, D) take one
+// stream-order transpose each, interleaved.  Lane l loads plane pl = (l ^ 7) & 15 of block
+// A / C (l < 16) or B / D (l >= 16), or in slot 15 that block's sign word, when that bit
+// of the block's plane mask k1 / k2 is set (sign-word offsets p1 / p2, `o` as in the
+// compressor: 0 for the sign word, 4 + 4 pl for a plane); afterwards lane e holds element
+// e of both blocks of a pair: magnitudes in bits 0-14 / 16-30, signs in bits 15 / 31.
+// Outlier mode: lane 0 replaces element 0's magnitude of a block whose head bit (hA..hD)
+// is set by the stored value (mA..mD).
+template <int MODE>
+__device__ __forceinline__ void decode_quad_1d_narrow(saddr_t pay, uint32_t k1, uint32_t p1, uint32_t k2, uint32_t p2,
+                                                      uint32_t pl, uint32_t o, uint32_t heads, uint32_t mA,
+                                                      uint32_t mB, uint32_t mC, uint32_t mD, int32_t& dA,
+                                                      int32_t& dB, int32_t& dC, int32_t& dD, int lane,
+                                                      const XposeLane& xl)
+{
+    uint32_t x1 = ((k1 >> pl) & 1u) ? lds32<MODE>(pay, p1 + o) : 0u;
+    uint32_t x2 = ((k2 >> pl) & 1u) ? lds32<MODE>(pay, p2 + o) : 0u;
+    warp_transpose32x2_stream(x1, x2, xl);
+    uint32_t a = x1 & 0x7fffu, b = (x1 >> 16) & 0x7fffu, c = x2 & 0x7fffu, d = (x2 >> 16) & 0x7fffu;
+    if constexpr (MODE == MODE_OUTLIER) {
+        if (lane == 0) {
+            if (heads & 1u) a = mA;
+            if (heads & 2u) b = mB;
+            if (heads & 4u) c = mC;
+            if (heads & 8u) d = mD;
+        }
+    }
+    dA = (x1 & 0x8000u) ? (int32_t)(0u - a) : (int32_t)a;
+    dB = (x1 & 0x80000000u) ? (int32_t)(0u - b) : (int32_t)b;
+    dC = (x2 & 0x8000u) ? (int32_t)(0u - c) : (int32_t)c;
+    dD = (x2 & 0x80000000u) ? (int32_t)(0u - d) : (int32_t)d;
+}
+
 // Two 2D/3D blocks at once: when both have payloads of rate <= 15 their transposes run
 // interleaved (signs included); otherwise one after the other.
 template <int MODE>
@@ -377,6 +410,51 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
     if (stored) bulk_wait_read();
     __syncwarp();
     if constexpr (DIM == 1) {
+        // every block with at most 15 planes (rate-0 blocks included): four blocks per
+        // step, each lane's block facts read by shuffles, no per-block rate arithmetic
+        uint32_t n1 = myr, ps1 = myo, m1 = 0, heads1 = 0;
+        if constexpr (MODE == MODE_OUTLIER) {
+            n1 = myr & 0x1fu;
+            const uint32_t ob1 = (myr & 0x80u) ? ((myr & 0x60u) >> 5) + 1u : 0u;
+            if (ob1) m1 = ld_outlier(pay, myo, ob1);
+            ps1 = myo + ob1;
+            heads1 = __ballot_sync(FULL, ob1 != 0);
+        }
+        if (__all_sync(FULL, lane >= C::BPW || n1 <= 15)) {
+            const uint32_t mask = plane_mask(myr, n1);
+            const uint32_t has = __ballot_sync(FULL, mysz != 0);   // bit j: block j has a payload
+            const int half = lane >> 4;
+            const uint32_t pl = (uint32_t)(lane ^ 7) & 15u;
+            const uint32_t o = pl == 15 ? 0u : 4u + 4u * pl;
+#pragma unroll 1
+            for (int j = 0; j < C::BPW; j += 4) {
+                const uint32_t k1 = __shfl_sync(FULL, mask, j + half), k2 = __shfl_sync(FULL, mask, j + 2 + half);
+                const uint32_t p1 = __shfl_sync(FULL, ps1, j + half), p2 = __shfl_sync(FULL, ps1, j + 2 + half);
+                uint32_t mA = 0, mB = 0, mC = 0, mD = 0;
+                if constexpr (MODE == MODE_OUTLIER) {
+                    mA = __shfl_sync(FULL, m1, j);
+                    mB = __shfl_sync(FULL, m1, j + 1);
+                    mC = __shfl_sync(FULL, m1, j + 2);
+                    mD = __shfl_sync(FULL, m1, j + 3);
+                }
+                int32_t dA, dB, dC, dD;
+                decode_quad_1d_narrow<MODE>(pay, k1, p1, k2, p2, pl, o, heads1 >> j, mA, mB, mC, mD, dA, dB, dC, dD,
+                                            lane, xl);
+                if constexpr (MODE != MODE_FIXED) {
+                    int32_t z = 0;
+                    lorenzo_inverse<1>(dA, z, lane);
+                    lorenzo_inverse<1>(dB, z, lane);
+                    lorenzo_inverse<1>(dC, z, lane);
+                    lorenzo_inverse<1>(dD, z, lane);
+                }
+                // blocks without payload decode to 0.0
+                const uint32_t hj = has >> j;
+                sts_val(obs + j * 32 * sizeof(T), (hj & 1u) ? dequant(dA, eb) : T(0));
+                sts_val(obs + (j + 1) * 32 * sizeof(T), (hj & 2u) ? dequant(dB, eb) : T(0));
+                sts_val(obs + (j + 2) * 32 * sizeof(T), (hj & 4u) ? dequant(dC, eb) : T(0));
+                sts_val(obs + (j + 3) * 32 * sizeof(T), (hj & 8u) ? dequant(dD, eb) : T(0));
+            }
+        } else
 #pragma unroll 1
         for (int j = 0; j < C::BPW; j += 2) {
             const uint32_t rA = __shfl_sync(FULL, myr, j), rB = __shfl_sync(FULL, myr, j + 1);
