@@ -402,6 +402,8 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 using namespace cuszp;
 
+extern "C" void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t p, cudaStream_t stream);
+
 struct cuszp_batch_plan {
     int count = 0;
     int dim = 1, type = 0;
@@ -409,8 +411,17 @@ struct cuszp_batch_plan {
     bool any_rel = false;
     int variant = 1;
     int ctas_per_sm = 0;       // 0: occupancy limit
+    bool configured = false;   // variant chosen by the autotuner or set_config
     bool tma_ok = false;       // every array suits the TMA kernels (variant 0)
     CUtensorMap* d_maps = nullptr;   // per-array tensor maps of the TMA kernels (2D/3D)
+    int cap_items = 0, cap_maps = 0; // device capacity of d_items / d_maps (arrays)
+    // pinned staging of the uploads (items, maps): the copies are truly asynchronous and
+    // never wait on the stream; `staged` marks when the last upload has read them
+    BatchItem* h_items = nullptr;
+    CUtensorMap* h_maps = nullptr;
+    int hcap_items = 0, hcap_maps = 0;
+    std::vector<void*> h_old;        // outgrown staging buffers, freed with the plan
+    cudaEvent_t staged = nullptr;
     std::vector<uint8_t> grouped;    // per array: its map is a grouped 2D map
     int sms = 148;
     std::vector<cuszp_batch_item_t> host_items;
@@ -421,6 +432,56 @@ struct cuszp_batch_plan {
     uint64_t total_tiles = 0, total_chunks = 0;
     size_t status_off = 0, map_off = 0, cmap_off = 0, part_off = 0;
 };
+
+// Pinned host memory of at least `n` elements of T for a staging buffer (grown by
+// doubling; an outgrown buffer is kept until the plan is destroyed, as freeing pinned
+// memory would synchronize the device).
+template <typename T>
+static int grow_pinned(cuszp_batch_plan* p, T** buf, int* cap, int n)
+{
+    if (n <= *cap) return OK;
+    const int want = std::max(n, 2 * *cap);
+    void* q = nullptr;
+    if (cudaHostAlloc(&q, sizeof(T) * (size_t)want, cudaHostAllocDefault) != cudaSuccess) return E_CUDA;
+    if (*buf) p->h_old.push_back(*buf);
+    *buf = static_cast<T*>(q);
+    *cap = want;
+    return OK;
+}
+
+// Device memory of at least `n` elements of T (grown by doubling, stream-ordered on s).
+template <typename T>
+static int grow_device(T** buf, int* cap, int n, cudaStream_t s)
+{
+    if (n <= *cap && *buf) return OK;
+    const int want = std::max(std::max(n, 1), 2 * *cap);
+    if (*buf) cudaFreeAsync(*buf, s);
+    *buf = nullptr;
+    *cap = 0;
+    if (cudaMallocAsync((void**)buf, sizeof(T) * (size_t)want, s) != cudaSuccess) return E_CUDA;
+    *cap = want;
+    return OK;
+}
+
+// The staging buffers are free once the previous upload has read them.
+static int stage_wait(cuszp_batch_plan* p)
+{
+    return p->staged && cudaEventSynchronize(p->staged) != cudaSuccess ? E_CUDA : OK;
+}
+
+// Uploads the item table through the pinned staging buffer.
+static int stage_items(cuszp_batch_plan* p, cudaStream_t s)
+{
+    int st = stage_wait(p);
+    if (!st) st = grow_pinned(p, &p->h_items, &p->hcap_items, p->count);
+    if (st) return st;
+    std::memcpy(p->h_items, p->items.data(), sizeof(BatchItem) * p->count);
+    if (cudaMemcpyAsync(p->d_items, p->h_items, sizeof(BatchItem) * p->count, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaEventRecord(p->staged, s) != cudaSuccess)
+        return E_CUDA;
+    return OK;
+}
 
 // (Re)builds the device item table, workspace and maps for a tile shape.  All
 // device work is stream-ordered on `s`; nothing here synchronizes the device.
@@ -466,10 +527,10 @@ static int plan_layout(cuszp_batch_plan* p, int variant, cudaStream_t s)
         p->ws_bytes = need;
     }
     if (cudaMemsetAsync(p->d_ws, 0, p->ws_bytes, s) != cudaSuccess) return E_CUDA;
-    // pageable source: staged before the call returns, so `items` may change afterwards
-    if (p->count && cudaMemcpyAsync(p->d_items, p->items.data(), sizeof(BatchItem) * p->count,
-                                    cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return E_CUDA;
+    if (p->count) {
+        int st = stage_items(p, s);
+        if (st) return st;
+    }
     char* ws = static_cast<char*>(p->d_ws);
     if (p->count)
         fill_maps_kernel<<<std::min(p->count, 4096), 256, 0, s>>>(p->d_items, p->count, (uint32_t*)(ws + p->map_off),
@@ -502,10 +563,14 @@ static int plan_maps(cuszp_batch_plan* p, cudaStream_t s)
         p->grouped[a] = grouped ? 1 : 0;
     }
     if (!p->tma_ok || maps.empty()) return OK;
-    if (cudaMallocAsync((void**)&p->d_maps, sizeof(CUtensorMap) * maps.size(), s) != cudaSuccess) return E_CUDA;
-    // pageable source: staged before the call returns
-    if (cudaMemcpyAsync(p->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, s) !=
-        cudaSuccess)
+    const int n = (int)maps.size();
+    int st = grow_device(&p->d_maps, &p->cap_maps, n, s);
+    if (!st) st = stage_wait(p);
+    if (!st) st = grow_pinned(p, &p->h_maps, &p->hcap_maps, n);
+    if (st) return st;
+    std::memcpy(p->h_maps, maps.data(), sizeof(CUtensorMap) * n);
+    if (cudaMemcpyAsync(p->d_maps, p->h_maps, sizeof(CUtensorMap) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaEventRecord(p->staged, s) != cudaSuccess)
         return E_CUDA;
     return OK;
 }
@@ -567,24 +632,41 @@ extern "C" int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count
         if (h.nbEle && (!h.d_in || !h.d_out)) { delete p; return E_ARG; }
         if (h.rel) p->any_rel = true;
     }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaMallocAsync((void**)&p->d_items, sizeof(BatchItem) * (count ? count : 1), stream) != cudaSuccess) {
-        delete p;
-        return E_CUDA;
-    }
-    int st = plan_maps(p, stream);
+    p->sms = std::max(1, sm_count());
+    int st = cudaEventCreateWithFlags(&p->staged, cudaEventDisableTiming) == cudaSuccess ? OK : E_CUDA;
+    if (!st) st = grow_device(&p->d_items, &p->cap_items, count, stream);
+    if (!st) st = plan_maps(p, stream);
     if (!st) st = plan_layout(p, p->tma_ok ? 0 : 1, stream);
     if (st) {
-        cudaFreeAsync(p->d_items, stream);
-        if (p->d_ws) cudaFreeAsync(p->d_ws, stream);
-        if (p->d_maps) cudaFreeAsync(p->d_maps, stream);
-        delete p;
+        cuSZp_batch_plan_destroy_async(p, stream);
         return st;
     }
     *plan = p;
     return OK;
+}
+
+extern "C" int cuSZp_batch_plan_update(cuszp_batch_plan_t p, int count, const cuszp_batch_item_t* items,
+                                       cudaStream_t stream)
+{
+    if (!p || count < 0 || (count && !items)) return E_ARG;
+    for (int a = 0; a < count; a++) {
+        const cuszp_batch_item_t& h = items[a];
+        if (h.mode < CUSZP_MODE_FIXED || h.mode > CUSZP_MODE_OUTLIER) return E_ARG;
+        if (h.nbEle && (!h.d_in || !h.d_out)) return E_ARG;
+    }
+    p->count = count;
+    p->host_items.assign(items, items + count);
+    p->items.resize(count);
+    p->any_rel = false;
+    for (int a = 0; a < count; a++)
+        if (items[a].rel) p->any_rel = true;
+    int st = grow_device(&p->d_items, &p->cap_items, count, stream);
+    if (!st) st = plan_maps(p, stream);
+    if (st) return st;
+    // a configured kernel pair is kept where the new arrays allow it; otherwise the default
+    int variant = p->configured ? p->variant : (p->tma_ok ? 0 : 1);
+    if (kVariants[variant].tma && !p->tma_ok) variant = 1;
+    return plan_layout(p, variant, stream);
 }
 
 extern "C" int cuSZp_batch_plan_create(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
@@ -665,6 +747,7 @@ extern "C" int cuSZp_batch_plan_tune(cuszp_batch_plan_t p, unsigned long long* d
     }
     int st = plan_layout(p, best_v, stream);
     p->ctas_per_sm = best_c;
+    p->configured = true;
     if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = E_CUDA;
     return st;
 }
@@ -675,6 +758,7 @@ extern "C" int cuSZp_batch_plan_set_config(cuszp_batch_plan_t p, int variant, in
     if (kVariants[variant].tma && !p->tma_ok) return E_UNSUPPORTED;
     const int st = plan_layout(p, variant, 0);
     p->ctas_per_sm = ctas_per_sm;
+    p->configured = true;
     if (st) return st;
     return cudaStreamSynchronize(0) == cudaSuccess ? OK : E_CUDA;
 }
@@ -685,6 +769,15 @@ extern "C" void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t p, cudaStream_
     if (p->d_items) cudaFreeAsync(p->d_items, stream);
     if (p->d_ws) cudaFreeAsync(p->d_ws, stream);
     if (p->d_maps) cudaFreeAsync(p->d_maps, stream);
+    // pinned staging: freed once the uploads that read it are done (freeing pinned
+    // memory waits for the device; a plan is destroyed outside any hot loop)
+    if (p->h_items || p->h_maps || !p->h_old.empty()) {
+        if (p->staged) cudaEventSynchronize(p->staged);
+        if (p->h_items) cudaFreeHost(p->h_items);
+        if (p->h_maps) cudaFreeHost(p->h_maps);
+        for (void* q : p->h_old) cudaFreeHost(q);
+    }
+    if (p->staged) cudaEventDestroy(p->staged);
     delete p;
 }
 

@@ -188,6 +188,31 @@ __device__ __forceinline__ uint32_t lds_u32(saddr_t a)
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
     return v;
 }
+// Stores and loads that take effect only where `c` holds, as predicated instructions:
+// lanes that skip them do not branch, so a warp whose lanes disagree does not diverge.
+__device__ __forceinline__ void sts_u32_if(bool c, saddr_t a, uint32_t v)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p st.shared.u32 [%0], %1;\n\t}"
+                 ::"r"(a), "r"(v), "r"((uint32_t)c) : "memory");
+}
+__device__ __forceinline__ void sts_u16_if(bool c, saddr_t a, uint32_t v)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p st.shared.u16 [%0], %1;\n\t}"
+                 ::"r"(a), "h"((unsigned short)v), "r"((uint32_t)c) : "memory");
+}
+__device__ __forceinline__ void sts_u8_if(bool c, saddr_t a, uint32_t v)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p st.shared.u8 [%0], %1;\n\t}"
+                 ::"r"(a), "r"(v), "r"((uint32_t)c) : "memory");
+}
+// 0 where `c` does not hold.
+__device__ __forceinline__ uint32_t lds_u32_if(bool c, saddr_t a)
+{
+    uint32_t v;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\tmov.u32 %0, 0;\n\t@p ld.shared.u32 %0, [%1];\n\t}"
+                 : "=r"(v) : "r"(a), "r"((uint32_t)c) : "memory");
+    return v;
+}
 // 16 bytes from a 16-byte aligned shared address.
 __device__ __forceinline__ uint4 lds_u128(saddr_t a)
 {

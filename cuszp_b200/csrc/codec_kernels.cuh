@@ -51,6 +51,27 @@ __device__ __forceinline__ void put32s(saddr_t a, uint32_t v)
         sts_u32(a, v);
     }
 }
+// put32s where `c` holds, without a branch on `c` (the outlier-mode byte offset's
+// residue mod 4 is uniform over a block's words, so its branch does not diverge there).
+template <int MODE>
+__device__ __forceinline__ void put32s_if(bool c, saddr_t a, uint32_t v)
+{
+    if constexpr (MODE == MODE_OUTLIER) {
+        const uint32_t r = a & 3u;
+        if (r == 0) {
+            sts_u32_if(c, a, v);
+        } else if (r == 2) {
+            sts_u16_if(c, a, v);
+            sts_u16_if(c, a + 2, v >> 16);
+        } else {
+            sts_u8_if(c, a, v);
+            sts_u16_if(c, a + 1, v >> 8);
+            sts_u8_if(c, a + 3, v >> 24);
+        }
+    } else {
+        sts_u32_if(c, a, v);
+    }
+}
 // Outlier-mode payload words sit at any byte offset: read the (at most two) aligned
 // words that hold the four bytes and funnel-shift.  Both aligned words contain bytes
 // of the payload itself, so the reads never leave the pages the stream occupies.
@@ -404,8 +425,8 @@ __device__ __forceinline__ void pack_quad_1d_narrow(int32_t cA, int32_t cB, int3
 {
     uint32_t x1 = slot_pair(cA, cB), x2 = slot_pair(cC, cD);
     warp_transpose32x2(x1, x2, xl);
-    if ((k1 >> pl) & 1u) put32s<MODE>(p1 + o, x1);
-    if ((k2 >> pl) & 1u) put32s<MODE>(p2 + o, x2);
+    put32s_if<MODE>((k1 >> pl) & 1u, p1 + o, x1);
+    put32s_if<MODE>((k2 >> pl) & 1u, p2 + o, x2);
 }
 
 // Payloads of two 2D/3D blocks of rate <= 15, sign words at pa / pb, transposes
@@ -423,8 +444,8 @@ __device__ __forceinline__ void pack_pair_narrow(uint32_t ka, uint32_t kb, int32
     const uint32_t pl = (lane ^ 7) & 15;
     const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
     const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
-    if ((ka >> pl) & 1u) put32s<MODE>(pa + o, xa);
-    if ((kb >> pl) & 1u) put32s<MODE>(pb + o, xb);
+    put32s_if<MODE>((ka >> pl) & 1u, pa + o, xa);
+    put32s_if<MODE>((kb >> pl) & 1u, pb + o, xb);
 }
 
 // Plane mask of a block for pack_pair_narrow (rate byte r, n <= 15 planes).

@@ -84,6 +84,19 @@ __device__ __forceinline__ uint32_t lds32(saddr_t p, uint32_t o)
         return lds_u32(p + o);
     }
 }
+// lds32 where `c` holds, 0 elsewhere, without a branch on `c`.
+template <int MODE>
+__device__ __forceinline__ uint32_t lds32_if(bool c, saddr_t p, uint32_t o)
+{
+    if constexpr (MODE == MODE_OUTLIER) {
+        const saddr_t w = p + (o & ~3u);
+        const uint32_t sh = (o & 3u) * 8;
+        const uint32_t lo = lds_u32_if(c, w), hi = lds_u32_if(c && sh, w + 4);
+        return sh ? __funnelshift_r(lo, hi, sh) : lo;
+    } else {
+        return lds_u32_if(c, p + o);
+    }
+}
 // Element 0's magnitude stored in `ob` (1..4) little-endian bytes at offset `o`: one
 // unaligned word read, masked (the bytes after it belong to the same payload).
 __device__ __forceinline__ uint32_t ld_outlier(saddr_t p, uint32_t o, uint32_t ob)
@@ -212,8 +225,8 @@ __device__ __forceinline__ void decode_pair_narrow(saddr_t pay, uint32_t pa, uin
     const uint32_t pl = (uint32_t)(lane ^ 7) & 15, h4 = (uint32_t)(lane >> 4) * 4;
     const uint32_t op = 8 + 8 * pl + h4;
     const uint32_t oa = pl < na ? op : h4, ob = pl < nb ? op : h4;
-    uint32_t xa = (pl < na || pl == 15) ? lds32<MODE>(pay, pa + oa) : 0u;
-    uint32_t xb = (pl < nb || pl == 15) ? lds32<MODE>(pay, pb + ob) : 0u;
+    uint32_t xa = lds32_if<MODE>(pl < na || pl == 15, pay, pa + oa);
+    uint32_t xb = lds32_if<MODE>(pl < nb || pl == 15, pay, pb + ob);
     warp_transpose32x2_stream(xa, xb, xl);
     uint32_t m0a = xa & 0x7fffu, m1a = (xa >> 16) & 0x7fffu, m0b = xb & 0x7fffu, m1b = (xb >> 16) & 0x7fffu;
     if constexpr (MODE == MODE_OUTLIER) {
@@ -243,8 +256,8 @@ __device__ __forceinline__ void decode_quad_1d_narrow(saddr_t pay, uint32_t k1, 
                                                       int32_t& dB, int32_t& dC, int32_t& dD, int lane,
                                                       const XposeLane& xl)
 {
-    uint32_t x1 = ((k1 >> pl) & 1u) ? lds32<MODE>(pay, p1 + o) : 0u;
-    uint32_t x2 = ((k2 >> pl) & 1u) ? lds32<MODE>(pay, p2 + o) : 0u;
+    uint32_t x1 = lds32_if<MODE>((k1 >> pl) & 1u, pay, p1 + o);
+    uint32_t x2 = lds32_if<MODE>((k2 >> pl) & 1u, pay, p2 + o);
     warp_transpose32x2_stream(x1, x2, xl);
     uint32_t a = x1 & 0x7fffu, b = (x1 >> 16) & 0x7fffu, c = x2 & 0x7fffu, d = (x2 >> 16) & 0x7fffu;
     if constexpr (MODE == MODE_OUTLIER) {

@@ -2,22 +2,26 @@
 
 Requests of mixed size, dtype, mode and dimensionality arrive over time.  Each loop
 iteration
-  1. retires finished batches (CUDA events), hands results out, returns their memory;
+  1. retires finished batches (CUDA events), hands their results out;
   2. admits arrived requests while the device-memory budget and the slot limit allow;
-  3. launches everything admitted but not yet started as ONE persistent batched
-     launch per (kind, dtype, dim) group -- on the next free stream, so batches
-     formed while others are still on the GPU overlap with them on the device.
-Every device step is stream-ordered (plan creation included); the host never
-synchronizes the device.  A request's result is byte-identical whether it runs
-alone or in any mix, because each array keeps its own look-back chain inside the
-batched kernel (cuszp_b200/csrc/batch.cu).
+  3. launches what was admitted as ONE persistent batched launch per (kind, dtype, dim)
+     group on the next free lane, so batches formed while others are still on the GPU
+     overlap with them on the device.
+State stays resident across batches: every lane keeps one batch plan per group
+(re-targeted with cuSZp_batch_plan_update: device tables and workspace are reused,
+uploads go through pinned staging memory) and its size buffers, and request outputs
+are carved out of one device arena of the budget's size, so the loop allocates no
+device memory and never synchronizes the device.  A request's result is
+byte-identical whether it runs alone or in any mix, because each array keeps its own
+look-back chain inside the batched kernel (cuszp_b200/csrc/batch.cu).
 """
 from __future__ import annotations
 
+import bisect
 import ctypes
 import time
 from collections import deque
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import torch
 
@@ -29,6 +33,8 @@ _P = ctypes.c_void_p
 lib.cuSZp_batch_plan_create_async.argtypes = [ctypes.POINTER(_P), ctypes.c_int, ctypes.POINTER(BatchItemC),
                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, _P]
 lib.cuSZp_batch_plan_create_async.restype = ctypes.c_int
+lib.cuSZp_batch_plan_update.argtypes = [_P, ctypes.c_int, ctypes.POINTER(BatchItemC), _P]
+lib.cuSZp_batch_plan_update.restype = ctypes.c_int
 lib.cuSZp_batch_plan_execute.argtypes = [_P, _P, _P]
 lib.cuSZp_batch_plan_execute.restype = ctypes.c_int
 lib.cuSZp_batch_plan_destroy_async.argtypes = [_P, _P]
@@ -51,7 +57,8 @@ class Request:
     done: float | None = None
     result: torch.Tensor | None = None   # compress: stream bytes [0,S); decompress: values
     size: int | None = None
-    mem: int = 0
+    mem: int = 0              # arena bytes held (output buffer)
+    off: int = -1             # arena offset of the output buffer
 
     @property
     def nbytes(self) -> int:
@@ -62,34 +69,92 @@ class Request:
         return Layout(self.n, self.dim, self.dims if self.dim != 1 else (0, 0, 0))
 
 
-@dataclass
-class _Batch:
-    event: torch.cuda.Event
-    stream: torch.cuda.Stream
-    requests: list
-    plans: list
-    sizes_host: torch.Tensor
-    sizes_dev: torch.Tensor
-    order: list = field(default_factory=list)
+class Arena:
+    """First-fit allocator over one device buffer (256-byte aligned blocks, adjacent free
+    blocks merged), so serving allocates no device memory per request."""
+
+    ALIGN = 256
+
+    def __init__(self, nbytes: int, device):
+        self.size = (nbytes + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        self.buf = torch.empty(self.size, dtype=torch.uint8, device=device)
+        self.starts = [0]            # free blocks, sorted by offset
+        self.lens = [self.size]
+        self.used = 0
+
+    def alloc(self, n: int) -> int:
+        n = max(self.ALIGN, (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN)
+        for i, ln in enumerate(self.lens):
+            if ln >= n:
+                off = self.starts[i]
+                if ln == n:
+                    del self.starts[i], self.lens[i]
+                else:
+                    self.starts[i] += n
+                    self.lens[i] -= n
+                self.used += n
+                return off
+        return -1
+
+    def free(self, off: int, n: int):
+        n = max(self.ALIGN, (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN)
+        self.used -= n
+        i = bisect.bisect_left(self.starts, off)
+        if i > 0 and self.starts[i - 1] + self.lens[i - 1] == off:        # merge with the block before
+            i -= 1
+            self.lens[i] += n
+        else:
+            self.starts.insert(i, off)
+            self.lens.insert(i, n)
+        if i + 1 < len(self.starts) and self.starts[i] + self.lens[i] == self.starts[i + 1]:   # and after
+            self.lens[i] += self.lens[i + 1]
+            del self.starts[i + 1], self.lens[i + 1]
+
+    @staticmethod
+    def rounded(n: int) -> int:
+        return max(Arena.ALIGN, (n + Arena.ALIGN - 1) // Arena.ALIGN * Arena.ALIGN)
+
+
+class _Lane:
+    """One stream with its resident batch plans (one per (kind, dtype, dim) group) and
+    size buffers; busy while a batch is on the GPU."""
+
+    def __init__(self, device, max_batch: int):
+        self.stream = torch.cuda.Stream(device)
+        self.plans: dict = {}
+        self.sizes_dev = torch.zeros(max_batch, dtype=torch.int64, device=device)
+        self.sizes_host = torch.zeros(max_batch, dtype=torch.int64, pin_memory=True)
+        self.event = torch.cuda.Event()
+        self.order: list = []
 
 
 class Server:
-    """Admission against `budget_bytes` of device memory (request outputs and plan
-    workspaces), at most `slots` requests in flight, at most `lanes` batches in flight."""
+    """Admission against `budget_bytes` of device memory (request outputs, carved from a
+    resident arena of that size), at most `slots` requests in flight, at most `lanes`
+    batches in flight.  Completed results are views into the arena: they stay valid
+    until `release(request)` returns their memory (or pass `consume` to `run`, which
+    releases each request after calling it)."""
 
-    def __init__(self, device=None, budget_bytes: int = 64 << 30, slots: int = 4096, lanes: int = 4,
+    def __init__(self, device=None, budget_bytes: int = 64 << 30, slots: int = 4096, lanes: int = 8,
                  max_batch: int = 1024):
         self.device = torch.device(device or "cuda")
-        self.budget = budget_bytes
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.arena = Arena(budget_bytes, self.device)
+        self.budget = self.arena.size
         self.slots = slots
         self.max_batch = max_batch
-        self.streams = deque(torch.cuda.Stream(self.device) for _ in range(lanes))
-        self.inflight: list[_Batch] = []
+        self.lanes = [_Lane(self.device, max_batch) for _ in range(lanes)]
+        self.free_lanes = deque(self.lanes)
+        self.inflight: list[_Lane] = []
         self.admitted: deque[Request] = deque()
-        self.used = 0
         self.active = 0
         self.launches = 0
         self.batches = 0
+
+    @property
+    def used(self) -> int:
+        return self.arena.used
 
     # ---------------------------------------------------------------- memory
 
@@ -99,103 +164,131 @@ class Server:
             return max(16, max_compressed_size(r.layout, r.dtype, r.mode))
         return r.nbytes
 
-    def _fits(self, r: Request) -> bool:
-        need = self._out_bytes(r) + 64 * 1024
-        return self.active < self.slots and self.used + need <= self.budget
+    def release(self, r: Request):
+        """Returns a completed request's output memory to the arena (its result view must
+        not be used afterwards)."""
+        if r.off >= 0:
+            self.arena.free(r.off, r.mem)
+            r.off, r.mem = -1, 0
 
     # ---------------------------------------------------------------- loop steps
 
     def admit(self, r: Request, now: float) -> bool:
-        if not self._fits(r):
+        if self.active >= self.slots:
             return False
-        r.mem = self._out_bytes(r) + 64 * 1024
-        self.used += r.mem
+        need = self._out_bytes(r)
+        off = self.arena.alloc(need)
+        if off < 0:
+            return False
+        r.off, r.mem = off, Arena.rounded(need)
         self.active += 1
         r.admitted = now
+        view = self.arena.buf[off: off + need]
         if r.kind == "compress":
-            r.result = torch.empty(self._out_bytes(r), dtype=torch.uint8, device=self.device)
+            r.result = view
         else:
             shape = (r.n,) if r.dim == 1 else (r.dims[2], r.dims[1], r.dims[0])
-            r.result = torch.empty(shape, dtype=r.dtype, device=self.device)
+            r.result = view.view(r.dtype).view(shape)
         self.admitted.append(r)
         return True
 
     def launch(self) -> bool:
-        if not self.admitted or not self.streams:
+        if not self.admitted or not self.free_lanes:
             return False
-        stream = self.streams.popleft()
+        lane = self.free_lanes.popleft()
         reqs = []
         while self.admitted and len(reqs) < self.max_batch:
             reqs.append(self.admitted.popleft())
         groups: dict = {}
         for r in reqs:
             groups.setdefault((r.kind, r.dtype, r.dim), []).append(r)
-        sizes_dev = torch.zeros(max(1, len(reqs)), dtype=torch.int64, device=self.device)
-        sizes_host = torch.zeros(max(1, len(reqs)), dtype=torch.int64, pin_memory=True)
-        plans, order, off = [], [], 0
+        stream = lane.stream
+        sp = _P(stream.cuda_stream)
+        order, off = [], 0
         with torch.cuda.stream(stream):
-            # inputs/outputs were produced on other streams
+            # inputs were produced on the default stream
             stream.wait_stream(torch.cuda.default_stream(self.device))
-            for (kind, dtype, dim), rs in groups.items():
+            for key, rs in groups.items():
+                kind, dtype, dim = key
                 arr = (BatchItemC * len(rs))()
                 for i, r in enumerate(rs):
-                    arr[i].d_in = r.data.data_ptr()
-                    arr[i].d_out = r.result.data_ptr()
-                    arr[i].nbEle = r.n
-                    arr[i].dims = Uint3(*r.layout.dims)
-                    arr[i].errorBound = r.eb
-                    arr[i].rel = 0
-                    arr[i].mode = MODES[r.mode]
-                h = _P()
-                st = lib.cuSZp_batch_plan_create_async(ctypes.byref(h), len(rs), arr, dim, TYPES[dtype],
-                                                       int(kind == "compress"), _P(stream.cuda_stream))
-                if st:
-                    raise CuszpError(st, "batch plan")
-                st = lib.cuSZp_batch_plan_execute(h, _P(sizes_dev.data_ptr() + 8 * off), _P(stream.cuda_stream))
+                    it = arr[i]
+                    it.d_in = r.data.data_ptr()
+                    it.d_out = r.result.data_ptr()
+                    it.nbEle = r.n
+                    it.dims = Uint3(*r.layout.dims)
+                    it.errorBound = r.eb
+                    it.rel = 0
+                    it.mode = MODES[r.mode]
+                h = lane.plans.get(key)
+                if h is None:
+                    h = _P()
+                    st = lib.cuSZp_batch_plan_create_async(ctypes.byref(h), len(rs), arr, dim, TYPES[dtype],
+                                                           int(kind == "compress"), sp)
+                    if st:
+                        raise CuszpError(st, "batch plan")
+                    lane.plans[key] = h
+                else:
+                    st = lib.cuSZp_batch_plan_update(h, len(rs), arr, sp)
+                    if st:
+                        raise CuszpError(st, "batch plan update")
+                st = lib.cuSZp_batch_plan_execute(h, _P(lane.sizes_dev.data_ptr() + 8 * off), sp)
                 if st:
                     raise CuszpError(st, "batch execute")
-                plans.append(h)
                 order.extend(rs)
                 off += len(rs)
                 self.launches += 1
-            sizes_host.copy_(sizes_dev, non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(stream)
+            lane.sizes_host[:off].copy_(lane.sizes_dev[:off], non_blocking=True)
+            lane.event.record(stream)
         for r in reqs:
             r.data.record_stream(stream)
-            r.result.record_stream(stream)
-        self.inflight.append(_Batch(ev, stream, order, plans, sizes_host, sizes_dev, order))
+        lane.order = order
+        self.inflight.append(lane)
         self.batches += 1
         return True
 
     def poll(self, now_fn) -> list:
         finished = []
         still = []
-        for b in self.inflight:
-            if b.event.query():
+        for lane in self.inflight:
+            if lane.event.query():
                 t = now_fn()
-                sizes = b.sizes_host.tolist()
-                for i, r in enumerate(b.order):
+                sizes = lane.sizes_host[: len(lane.order)].tolist()
+                for i, r in enumerate(lane.order):
                     if r.kind == "compress":
                         r.size = int(sizes[i])
                         r.result = r.result[: r.size]
+                        # the unused tail of the worst-case buffer goes back to the arena
+                        keep = Arena.rounded(r.size)
+                        if keep < r.mem:
+                            self.arena.free(r.off + keep, r.mem - keep)
+                            r.mem = keep
                     r.done = t
-                    self.used -= r.mem
                     self.active -= 1
                     finished.append(r)
-                for h in b.plans:
-                    lib.cuSZp_batch_plan_destroy_async(h, _P(b.stream.cuda_stream))
-                self.streams.append(b.stream)
+                lane.order = []
+                self.free_lanes.append(lane)
             else:
-                still.append(b)
+                still.append(lane)
         self.inflight = still
         return finished
 
+    def close(self):
+        """Waits for the lanes and destroys their plans."""
+        for lane in self.lanes:
+            lane.stream.synchronize()
+            for h in lane.plans.values():
+                lib.cuSZp_batch_plan_destroy_async(h, _P(lane.stream.cuda_stream))
+            lane.plans.clear()
+        torch.cuda.synchronize(self.device)
+
     # ---------------------------------------------------------------- driver
 
-    def run(self, requests: list, open_loop: bool = True, idle_sleep: float = 20e-6) -> dict:
+    def run(self, requests: list, open_loop: bool = True, idle_sleep: float = 20e-6, consume=None) -> dict:
         """Serve `requests` (sorted by arrival).  open_loop: requests become visible at
-        their arrival time; otherwise all are available at t = 0."""
+        their arrival time; otherwise all are available at t = 0.  consume(r), when
+        given, is called as each request completes, after which its output memory is
+        released (the result view is then invalid)."""
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         t0 = time.perf_counter()
 
@@ -206,18 +299,29 @@ class Server:
         total = len(requests)
         while done < total:
             t = now()
-            done += len(self.poll(now))
+            fin = self.poll(now)
+            done += len(fin)
+            if consume is not None:
+                for r in fin:
+                    consume(r)
+                    self.release(r)
+            blocked = False
             while pending and (not open_loop or pending[0].arrival <= t):
                 if not self.admit(pending[0], t):
+                    blocked = True
                     break
                 pending.popleft()
-            launched = self.launch()
-            if not launched and not self.inflight and pending and open_loop:
+            if self.launch():
+                continue
+            if self.inflight:
+                time.sleep(idle_sleep)
+            elif blocked and not self.admitted:
+                # nothing in flight and the next request still does not fit
+                raise RuntimeError("request does not fit the memory budget (results not released?)")
+            elif pending and open_loop:
                 wait = pending[0].arrival - now()
                 if wait > 0:
                     time.sleep(min(wait, 1e-3))
-            elif not launched:
-                time.sleep(idle_sleep)
         torch.cuda.synchronize(self.device)
         wall = now()
         return summarize(requests, wall, extra={"launches": self.launches, "batches": self.batches})
@@ -266,9 +370,11 @@ def summarize(requests: list, wall: float, extra: dict | None = None) -> dict:
         return lat[k] * 1e3
 
     nbytes = sum(r.nbytes for r in requests)
+    waits = sorted((r.admitted - r.arrival) for r in requests if r.admitted is not None)
     out = {"requests": len(requests), "wall_s": wall, "throughput_gbs": nbytes / wall / 1e9 if wall > 0 else None,
            "req_per_s": len(requests) / wall if wall > 0 else None, "p50_ms": pct(50), "p99_ms": pct(99),
-           "p999_ms": pct(99.9), "bytes": nbytes}
+           "p999_ms": pct(99.9), "bytes": nbytes,
+           "admit_wait_p99_ms": waits[min(len(waits) - 1, int(round(0.99 * (len(waits) - 1))))] * 1e3 if waits else None}
     if extra:
         out.update(extra)
     return out
@@ -353,6 +459,10 @@ def make_requests(count: int, rate: float, pools: dict, seed: int = 4, min_bytes
 
 
 def reset(requests: list):
+    """Clears the per-run fields of requests whose outputs were released (or never came
+    from a server's arena), so they can be served again."""
     for r in requests:
+        if r.off >= 0:
+            raise ValueError(f"request {r.rid} still holds arena memory: release it first")
         r.admitted = r.done = r.result = r.size = None
         r.mem = 0

@@ -186,6 +186,14 @@ int cuSZp_batch_plan_create(cuszp_batch_plan_t* plan, int count, const cuszp_bat
  * work in flight. */
 int cuSZp_batch_plan_create_async(cuszp_batch_plan_t* plan, int count, const cuszp_batch_item_t* items,
                                   cuszp_dim_t dim, cuszp_type_t type, int compress, cudaStream_t stream);
+/* Re-targets a plan at a new list of arrays (same dim, type and direction), reusing its
+ * device buffers (grown when the new list needs more) and its pinned staging memory, so
+ * a request loop keeps one plan per lane instead of creating and destroying one per
+ * batch.  Stream-ordered on `stream`, no device synchronization; work that still uses
+ * the plan must be ordered before `stream`.  The kernel pair chosen for the plan is kept
+ * where the new arrays allow it. */
+int cuSZp_batch_plan_update(cuszp_batch_plan_t plan, int count, const cuszp_batch_item_t* items,
+                            cudaStream_t stream);
 /* Enqueue the batch on `stream`; stream lengths go to d_sizes[count] (device u64). */
 int cuSZp_batch_plan_execute(cuszp_batch_plan_t plan, unsigned long long* d_sizes, cudaStream_t stream);
 /* Autotuner: time each tile shape (warps per CTA x blocks per warp) and CTAs per SM on

@@ -20,9 +20,14 @@ def test_mixed_requests_identical_alone_and_in_the_mix():
     from cuszp_b200 import serve
     pools = serve.make_pools(torch.device("cuda"), max_bytes=8 << 20)
     reqs = serve.make_requests(120, rate=20000.0, pools=pools, seed=7, max_bytes=8 << 20, stream_pool=12)
-    # a tight budget forces admission to wait for memory to free up
+    # a tight budget forces admission to wait for memory to free up: each result is
+    # copied out as it completes and its arena memory released
     srv = serve.Server(budget_bytes=48 << 20, lanes=3, max_batch=16)
-    stats = srv.run(reqs, open_loop=True)
+
+    def consume(r):
+        r.result = r.result.clone()
+
+    stats = srv.run(reqs, open_loop=True, consume=consume)
     assert stats["requests"] == 120 and srv.active == 0 and srv.used == 0
     assert srv.batches > 1
     kinds = {r.kind for r in reqs}
@@ -42,9 +47,48 @@ def test_sequential_baseline_gives_the_same_bytes():
     from cuszp_b200 import serve
     pools = serve.make_pools(torch.device("cuda"), max_bytes=4 << 20)
     reqs = serve.make_requests(30, rate=0.0, pools=pools, seed=9, max_bytes=4 << 20, stream_pool=6)
-    serve.Server(lanes=2, max_batch=8).run(reqs, open_loop=False)
+    srv = serve.Server(budget_bytes=256 << 20, lanes=2, max_batch=8)
+    srv.run(reqs, open_loop=False)
     batched = [r.result.clone() for r in reqs]
+    for r in reqs:
+        srv.release(r)
+    assert srv.used == 0
+    srv.close()
     serve.reset(reqs)
     serve.serve_sequential(reqs, open_loop=False)
     for r, b in zip(reqs, batched):
         assert torch.equal(r.result.reshape(-1).view(torch.uint8), b.reshape(-1).view(torch.uint8)), r.rid
+
+
+def test_resident_plans_are_reused_across_batches():
+    """Lanes keep one plan per (kind, dtype, dim) group and re-target it: later batches
+    create no plans, and outputs still match the requests served alone."""
+    from cuszp_b200 import serve
+    pools = serve.make_pools(torch.device("cuda"), max_bytes=2 << 20)
+    reqs = serve.make_requests(80, rate=0.0, pools=pools, seed=11, max_bytes=2 << 20, stream_pool=8)
+    srv = serve.Server(budget_bytes=512 << 20, lanes=2, max_batch=4)
+    srv.run(reqs, open_loop=False)
+    plans = sum(len(lane.plans) for lane in srv.lanes)
+    assert srv.batches >= 20 and plans <= 2 * 18
+    for r in reqs:
+        ref = _alone(r)
+        if r.kind == "compress":
+            assert torch.equal(r.result, ref), r.rid
+        else:
+            assert torch.equal(r.result.reshape(-1).view(torch.uint8), ref.reshape(-1).view(torch.uint8)), r.rid
+        srv.release(r)
+    assert srv.used == 0
+    srv.close()
+
+
+def test_arena_first_fit_merges_free_blocks():
+    from cuszp_b200.serve import Arena
+    a = Arena(4096, torch.device("cuda"))
+    x, y, z = a.alloc(1000), a.alloc(1000), a.alloc(1000)
+    assert (x, y, z) == (0, 1024, 2048) and a.alloc(2048) == -1
+    a.free(y, 1000)
+    a.free(x, 1000)
+    assert a.alloc(2048) == 0               # the two freed neighbours merged
+    a.free(0, 2048)
+    a.free(z, 1000)
+    assert a.used == 0 and a.starts == [0] and a.lens == [4096]
