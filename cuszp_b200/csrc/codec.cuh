@@ -266,9 +266,13 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int row)
 
 // The per-lane constants of the five butterfly stages for a fixed row index, for loops
 // that transpose many words with the same row: keep mask and rotate amount per stage.
+// The two whole-byte stages (distances 16 and 8) keep / take whole bytes, so each is one
+// byte permute of the lane's and its partner's word (selectors byte16 / byte8) instead
+// of a rotate and a masked merge.
 struct XposeLane {
     uint32_t keep[5];
     uint32_t rot[5];
+    uint32_t byte16, byte8;
     __device__ __forceinline__ explicit XposeLane(int row)
     {
 #pragma unroll
@@ -280,6 +284,20 @@ struct XposeLane {
             keep[i] = up ? m : ~m;
             rot[i] = up ? (uint32_t)j : (uint32_t)(32 - j);
         }
+        // __byte_perm(x, y, s): selector nibble n picks result byte n from x (0-3) or y (4-7).
+        // distance 16: upper lanes keep x's high half and take y's high half as their low
+        // half; lower lanes keep x's low half and take y's low half as their high half.
+        byte16 = (row & 16) ? 0x3276u : 0x5410u;
+        // distance 8: upper lanes keep x's odd bytes and take y's odd bytes into the even
+        // positions; lower lanes keep x's even bytes and take y's even bytes into the odd ones.
+        byte8 = (row & 8) ? 0x3715u : 0x6240u;
+    }
+    // One butterfly stage i (distance 16 >> i) of word x with its partner's word y.
+    __device__ __forceinline__ uint32_t stage(int i, uint32_t x, uint32_t y) const
+    {
+        if (i == 0) return __byte_perm(x, y, byte16);
+        if (i == 1) return __byte_perm(x, y, byte8);
+        return (x & keep[i]) | (__funnelshift_r(y, y, rot[i]) & ~keep[i]);
     }
 };
 // Two independent transposes, interleaved stage by stage (twice the work per dependent
@@ -291,8 +309,8 @@ __device__ __forceinline__ void warp_transpose32x2(uint32_t& a, uint32_t& b, con
         const int j = 16 >> i;
         const uint32_t ya = __shfl_xor_sync(FULL, a, j);
         const uint32_t yb = __shfl_xor_sync(FULL, b, j);
-        a = (a & xl.keep[i]) | (__funnelshift_r(ya, ya, xl.rot[i]) & ~xl.keep[i]);
-        b = (b & xl.keep[i]) | (__funnelshift_r(yb, yb, xl.rot[i]) & ~xl.keep[i]);
+        a = xl.stage(i, a, ya);
+        b = xl.stage(i, b, yb);
     }
 }
 // Two transposes of stream-order words, for the decoder: lane l holds the word of row
@@ -309,8 +327,8 @@ __device__ __forceinline__ void warp_transpose32x2_stream(uint32_t& a, uint32_t&
         const uint32_t ya = __shfl_xor_sync(FULL, a, j);
         const uint32_t yb = __shfl_xor_sync(FULL, b, j);
         if (i < 2) {
-            a = (a & xl.keep[i]) | (__funnelshift_r(ya, ya, xl.rot[i]) & ~xl.keep[i]);
-            b = (b & xl.keep[i]) | (__funnelshift_r(yb, yb, xl.rot[i]) & ~xl.keep[i]);
+            a = xl.stage(i, a, ya);
+            b = xl.stage(i, b, yb);
         } else {
             a = (a & ~xl.keep[i]) | (__funnelshift_l(ya, ya, xl.rot[i]) & xl.keep[i]);
             b = (b & ~xl.keep[i]) | (__funnelshift_l(yb, yb, xl.rot[i]) & xl.keep[i]);
@@ -323,7 +341,7 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, const XposeLane
     for (int i = 0; i < 5; i++) {
         const int j = 16 >> i;
         const uint32_t y = __shfl_xor_sync(FULL, x, j);
-        x = (x & xl.keep[i]) | (__funnelshift_r(y, y, xl.rot[i]) & ~xl.keep[i]);
+        x = xl.stage(i, x, y);
     }
     return x;
 }
