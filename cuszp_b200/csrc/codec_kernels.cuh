@@ -243,6 +243,101 @@ __device__ __forceinline__ void lorenzo_inverse(int32_t& d0, int32_t& d1, int la
     }
 }
 
+// The same inverse with the lane-dependent parts precomputed per lane as 0/1
+// multipliers: every conditional add of the prefix sums is one multiply-add (the FMA
+// pipe) instead of a compare and a predicated add (the ALU pipe, which the decoders
+// saturate).  Integer arithmetic wraps as in lorenzo_inverse.
+template <int DIM>
+struct LorenzoLane {
+    uint32_t mx[DIM == 1 ? 5 : DIM == 2 ? 3 : 2];   // x-direction prefix steps (1D: all five)
+    uint32_t my[2];                                 // 2D: rows, 3D: row starts
+    uint32_t first;                                 // 2D: column 0, 3D: row start (x == 0)
+    uint32_t hi;                                    // 3D: second half of the block (z >= 2)
+    __device__ __forceinline__ explicit LorenzoLane(int lane)
+    {
+        if constexpr (DIM == 1) {
+#pragma unroll
+            for (int i = 0; i < 5; i++) mx[i] = lane >= (1 << i) ? 1u : 0u;
+            my[0] = my[1] = first = hi = 0;
+        } else if constexpr (DIM == 2) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) mx[i] = (lane & 7) >= (1 << i) ? 1u : 0u;
+            my[0] = lane >= 8 ? 1u : 0u;
+            my[1] = lane >= 16 ? 1u : 0u;
+            first = (lane & 7) == 0 ? 1u : 0u;
+            hi = 0;
+        } else {
+            mx[0] = (lane & 3) >= 1 ? 1u : 0u;
+            mx[1] = (lane & 3) >= 2 ? 1u : 0u;
+            my[0] = (lane & 15) >= 4 ? 1u : 0u;
+            my[1] = (lane & 15) >= 8 ? 1u : 0u;
+            first = (lane & 3) == 0 ? 1u : 0u;
+            hi = lane >= 16 ? 1u : 0u;
+        }
+    }
+};
+
+// d + t * m with wrapping 32-bit arithmetic (m is 0 or 1).
+__device__ __forceinline__ int32_t madd(int32_t d, int32_t t, uint32_t m)
+{
+    return (int32_t)((uint32_t)d + (uint32_t)t * m);
+}
+
+template <int DIM>
+__device__ __forceinline__ void lorenzo_inverse(int32_t& d0, int32_t& d1, int lane, const LorenzoLane<DIM>& L)
+{
+    if constexpr (DIM == 1) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) d0 = madd(d0, __shfl_up_sync(FULL, d0, 1 << i), L.mx[i]);
+    } else if constexpr (DIM == 2) {
+        int32_t r0 = d0, r1 = d1;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const int32_t t0 = __shfl_up_sync(FULL, r0, 1 << i), t1 = __shfl_up_sync(FULL, r1, 1 << i);
+            r0 = madd(r0, t0, L.mx[i]);
+            r1 = madd(r1, t1, L.mx[i]);
+        }
+        const int32_t v0 = (int32_t)((uint32_t)d0 * L.first), v1 = (int32_t)((uint32_t)d1 * L.first);
+        int32_t i0 = v0, i1 = v1;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int32_t t0 = __shfl_up_sync(FULL, i0, 8 << i), t1 = __shfl_up_sync(FULL, i1, 8 << i);
+            i0 = madd(i0, t0, L.my[i]);
+            i1 = madd(i1, t1, L.my[i]);
+        }
+        const int32_t tot0 = __shfl_sync(FULL, i0, 24);
+        const int32_t e0 = __shfl_sync(FULL, wsub(i0, v0), lane & 24);
+        const int32_t e1 = __shfl_sync(FULL, wsub(i1, v1), lane & 24);
+        d0 = wadd(r0, e0);
+        d1 = wadd(wadd(r1, e1), tot0);
+    } else {
+        int32_t x0 = d0, x1 = d1;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int32_t t0 = __shfl_up_sync(FULL, x0, 1 << i), t1 = __shfl_up_sync(FULL, x1, 1 << i);
+            x0 = madd(x0, t0, L.mx[i]);
+            x1 = madd(x1, t1, L.mx[i]);
+        }
+        const int32_t v0 = (int32_t)((uint32_t)d0 * L.first), v1 = (int32_t)((uint32_t)d1 * L.first);
+        int32_t y0 = v0, y1 = v1;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int32_t t0 = __shfl_up_sync(FULL, y0, 4 << i), t1 = __shfl_up_sync(FULL, y1, 4 << i);
+            y0 = madd(y0, t0, L.my[i]);
+            y1 = madd(y1, t1, L.my[i]);
+        }
+        const int32_t zs0 = __shfl_sync(FULL, d0, 0);
+        const int32_t zs1 = wadd(zs0, __shfl_sync(FULL, d0, 16));
+        const int32_t zs2 = wadd(zs1, __shfl_sync(FULL, d1, 0));
+        const int32_t E0 = (int32_t)((uint32_t)zs0 * L.hi);
+        const int32_t E1 = madd(zs1, wsub(zs2, zs1), L.hi);
+        const int32_t b0 = __shfl_sync(FULL, wsub(wadd(E0, y0), v0), lane & ~3);
+        const int32_t b1 = __shfl_sync(FULL, wsub(wadd(E1, y1), v1), lane & ~3);
+        d0 = wadd(x0, b0);
+        d1 = wadd(x1, b1);
+    }
+}
+
 // --------------------------------------------------------------- compress phases
 
 template <typename T, int DIM, typename Tl>

@@ -340,6 +340,7 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
     using C = DecCfg<T, DIM>;
     const Geom g = *A.g;
     const T eb = src.eb_of(A);
+    const LorenzoLane<DIM> ll(lane);
     T* out = static_cast<T*>(A.data);
     const bool bad = sh.poff[f] == kBadSlot;
     // this warp's blocks: rate bytes, payload offsets (lane j: block j)
@@ -404,8 +405,8 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             bool za, zb;
             decode(j, d0a, d1a, d0b, d1b, za, zb);
             if constexpr (MODE != MODE_FIXED) {
-                lorenzo_inverse<DIM>(d0a, d1a, lane);
-                lorenzo_inverse<DIM>(d0b, d1b, lane);
+                lorenzo_inverse<DIM>(d0a, d1a, lane, ll);
+                lorenzo_inverse<DIM>(d0b, d1b, lane, ll);
             }
             if (q) {
                 T* qa = q + (uint32_t)j * 8;
@@ -455,10 +456,10 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
                                             lane, xl);
                 if constexpr (MODE != MODE_FIXED) {
                     int32_t z = 0;
-                    lorenzo_inverse<1>(dA, z, lane);
-                    lorenzo_inverse<1>(dB, z, lane);
-                    lorenzo_inverse<1>(dC, z, lane);
-                    lorenzo_inverse<1>(dD, z, lane);
+                    lorenzo_inverse<1>(dA, z, lane, ll);
+                    lorenzo_inverse<1>(dB, z, lane, ll);
+                    lorenzo_inverse<1>(dC, z, lane, ll);
+                    lorenzo_inverse<1>(dD, z, lane, ll);
                 }
                 // blocks without payload decode to 0.0
                 const uint32_t hj = has >> j;
@@ -476,8 +477,8 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             decode_pair_1d<MODE>(pay, rA, rB, oA, oB, dA, dB, lane, xl);
             if constexpr (MODE != MODE_FIXED) {
                 int32_t z = 0;
-                lorenzo_inverse<1>(dA, z, lane);
-                lorenzo_inverse<1>(dB, z, lane);
+                lorenzo_inverse<1>(dA, z, lane, ll);
+                lorenzo_inverse<1>(dB, z, lane, ll);
             }
             // blocks without payload decode to 0.0
             sts_val(obs + j * 32 * sizeof(T), payload_size<1, MODE>(rA) ? dequant(dA, eb) : T(0));
@@ -490,8 +491,8 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             bool za, zb;
             decode(j, d0a, d1a, d0b, d1b, za, zb);
             if constexpr (MODE != MODE_FIXED) {
-                lorenzo_inverse<DIM>(d0a, d1a, lane);
-                lorenzo_inverse<DIM>(d0b, d1b, lane);
+                lorenzo_inverse<DIM>(d0a, d1a, lane, ll);
+                lorenzo_inverse<DIM>(d0b, d1b, lane, ll);
             }
             const saddr_t oj = obs + j * 64 * sizeof(T);
             sts_val(oj, za ? T(0) : dequant(d0a, eb));
