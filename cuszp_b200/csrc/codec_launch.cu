@@ -330,7 +330,10 @@ static KernelRef dtma_kernel_for(const Problem& p, bool grouped)
     return dtma_pick<double, 3>(p.mode);
 }
 
-// CUSZP_TICKET_TILES=1..4 in the environment fixes the TMA decompress kernel's tiles per
+// Tiles per decompress ticket chosen for large arrays.
+constexpr int kTicketTiles = 4;
+
+// CUSZP_TICKET_TILES=1..16 in the environment fixes the TMA decompress kernel's tiles per
 // ticket (0: the size-based choice) -- for tests of both ticket forms on small arrays.
 static int ticket_tiles_override()
 {
@@ -361,10 +364,11 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     float ebf = (float)eb;
     void* dst = out;
     const void* src = cmp;
-    // f64 tiles (32 KB of output) decode fast enough that the look-back chain limits:
-    // tickets of kMaxTicketTiles tiles when every front warp still gets two of them
+    // the look-back chain limits once decoding is fast: tickets of kTicketTiles tiles
+    // when every front warp still gets two of them (measured on 512^3 f32 3D and 8192^2 f64
+    // 2D: 4 tiles beat 1, 2, 3, 8 and 16; small arrays keep single-tile tickets)
     const uint64_t front = (uint64_t)grid * (k.threads / 32 - DecCfg<double, 1>::WARPS);   // front warps
-    int tickets = p.type == 1 && p.g.ntiles >= 2ull * kMaxTicketTiles * front ? kMaxTicketTiles : 1;
+    int tickets = p.g.ntiles >= 2ull * kTicketTiles * front ? kTicketTiles : 1;
     if (const int forced = ticket_tiles_override()) tickets = forced;
     void* args[] = {(void*)&map, (void*)&dst, (void*)&src, (void*)&g, p.type == 0 ? (void*)&ebf : (void*)&eb,
                     (void*)&hdr, (void*)&status, (void*)&tickets};

@@ -52,7 +52,7 @@ struct DecCfg {
 };
 
 constexpr uint32_t kBadSlot = 0xffffffffu;   // poff of a tile whose rate bytes are invalid
-constexpr int kMaxTicketTiles = 4;           // decompress: most tiles per ticket (one look-back each)
+constexpr int kMaxTicketTiles = 16;          // decompress: most tiles per ticket (one look-back each)
 
 template <typename T, int DIM>
 struct DecShared {
@@ -572,17 +572,41 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
         const int f = warp - C::WARPS;
         uint8_t* slot = slots + f * C::SLOT;
         // A ticket is a group of G consecutive tiles of one array (G = Src::ticket_tiles(),
-        // up to kMaxTicketTiles for f64, 1 for f32): their rate bytes give every tile's
-        // payload size at once, and one status word per group carries the look-back, so
-        // the chain of inclusive prefixes advances G tiles per step.  The group's tiles
-        // then fill the slot one after another.  Fill m is prepared while the codec warps
-        // still decode fill m - 1; only its payload load waits for the slot.
-        constexpr int GM = sizeof(T) == 8 ? kMaxTicketTiles : 1;   // f32 tickets stay single tiles
+        // up to kMaxTicketTiles): their rate bytes give the group's payload size at once,
+        // and one status word per group carries the look-back, so the chain of inclusive
+        // prefixes advances G tiles per step.  The group's tiles then fill the slot one
+        // after another (their rate bytes read again, from the cache).  Fill m is prepared
+        // while the codec warps still decode fill m - 1; only its payload load waits for
+        // the slot.
         constexpr int PER = C::TB / 32;   // rate bytes per lane and tile (4 in 1D, 2 in 2D/3D)
         constexpr int LPW = C::BPW / PER; // lanes per codec warp
-        const int G = min(src.ticket_tiles(), GM);
+        const int G = max(1, min(src.ticket_tiles(), kMaxTicketTiles));
         int m = 0;                        // fills of the slot so far
         bool failed = false;              // left after a wait gave up
+        // A tile's rate bytes (this lane's PER consecutive blocks): block sizes, their sum,
+        // and the warp-exclusive prefix of the sums (where this lane's blocks start).
+        auto tile_sizes = [&](const TileArray& A, const Geom& g, int64_t lt, uint32_t* rb, uint32_t& lane_off,
+                              uint32_t& total) {
+            const uint64_t b0 = (uint64_t)lt * C::TB;
+            uint32_t rsum = 0;
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                const uint64_t b = b0 + (uint64_t)lane * PER + e;   // lane holds consecutive blocks
+                const uint32_t r = b < g.nblocks ? __ldg(A.cmp + b) : 0u;
+                rb[e] = r;
+                uint32_t sz = 0;
+                src.with_mode(A.mode, [&](auto md) { sz = payload_size<DIM, decltype(md)::value>(r); });
+                rsum += sz;
+            }
+            uint32_t incl = rsum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            lane_off = incl - rsum;
+            total = __shfl_sync(FULL, incl, 31);
+        };
         for (;;) {
             int64_t gi = 0;
             if (lane == 0) gi = (int64_t)atomicAdd(&hdr->ticket, 1u);
@@ -605,31 +629,13 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
             const uint8_t* cmp = A.cmp;
             unsigned long long* status = A.status;
             const int64_t grp = lt0 / G;   // status word of the group
-            // rate bytes -> block sizes -> per tile: warp offsets and aggregate
-            uint32_t rbyte[GM][PER], wo[GM], agg[GM];
+            // the group's payload bytes: every tile's rate bytes -> sizes -> sum (the group's
+            // tiles are read again as they fill the slot, from the cache)
             unsigned long long gagg = 0;
-#pragma unroll
-            for (int i = 0; i < GM; i++) {
-                const uint64_t b0 = (uint64_t)(lt0 + i) * C::TB;
-                uint32_t rsum = 0;
-#pragma unroll
-                for (int e = 0; e < PER; e++) {
-                    const uint64_t b = b0 + (uint64_t)lane * PER + e;   // lane holds consecutive blocks
-                    const uint32_t r = i < n && b < g.nblocks ? __ldg(cmp + b) : 0u;
-                    rbyte[i][e] = r;
-                    uint32_t sz = 0;
-                    src.with_mode(A.mode, [&](auto md) { sz = payload_size<DIM, decltype(md)::value>(r); });
-                    rsum += sz;
-                }
-                uint32_t incl = rsum;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t v = __shfl_up_sync(FULL, incl, o);
-                    if (lane >= o) incl += v;
-                }
-                wo[i] = incl - rsum;
-                agg[i] = __shfl_sync(FULL, incl, 31);
-                gagg += agg[i];
+            for (int i = 0; i < n; i++) {
+                uint32_t rb[PER], lo, tot;
+                tile_sizes(A, g, lt0 + i, rb, lo, tot);
+                gagg += tot;
             }
             if (lane == 0) st_post(status + grp, (grp == 0 ? ST_INC : ST_AGG) | gagg);
             const uint64_t excl = grp > 0 ? warp_lookback(status, grp, err) : 0;
@@ -639,20 +645,20 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
             }
             uint64_t p0 = g.rate_bytes + excl;   // payload start of the group's next tile
             bool stop = false;
-#pragma unroll
-            for (int i = 0; i < GM; i++) {
-                if (i >= n) break;
+            for (int i = 0; i < n; i++) {
                 const int rb = m & 1;
+                uint32_t rbyte[PER], wo, agg;
+                tile_sizes(A, g, lt0 + i, rbyte, wo, agg);
 #pragma unroll
-                for (int e = 0; e < PER; e++) sh.rates[f][rb][lane * PER + e] = (uint8_t)rbyte[i][e];
-                if (lane % LPW == 0) sh.woff[f][rb][lane / LPW] = wo[i];
-                const uint64_t p1 = p0 + agg[i];
+                for (int e = 0; e < PER; e++) sh.rates[f][rb][lane * PER + e] = (uint8_t)rbyte[e];
+                if (lane % LPW == 0) sh.woff[f][rb][lane / LPW] = wo;
+                const uint64_t p1 = p0 + agg;
                 const uint64_t a0 = p0 & ~15ull, a1 = (p1 + 15) & ~15ull;
                 // rate bytes no valid stream holds (rate > 32 outside outlier mode) could
                 // claim more than a slot: such a tile is not loaded and decodes to zeros
-                const bool fits = agg[i] <= (uint32_t)(C::TB * C::MAXBLK);
+                const bool fits = agg <= (uint32_t)(C::TB * C::MAXBLK);
                 if (!fits && lane == 0) atomicOr(err, ERR_CAPACITY);
-                const uint32_t bytes = agg[i] && fits ? (uint32_t)(a1 - a0) : 0u;
+                const uint32_t bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
                 // the slot: fill m - 1 decoded
                 if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) { stop = true; break; }
                 __syncwarp();   // rates and offsets are written before lane 0 publishes the fill

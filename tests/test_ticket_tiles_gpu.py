@@ -1,9 +1,9 @@
 """The TMA decompress kernel's grouped tickets (several consecutive tiles per ticket,
-one look-back status word per group): forced on small f64 arrays through
-CUSZP_TICKET_TILES (the size-based choice takes them only for large f64 arrays; f32
-kernels keep single-tile tickets), the reconstructions must stay identical to the
-oracle's, including groups cut short by the last tile.  The library reads the variable
-once, so the decompressions run in a child process per ticket size."""
+one look-back status word per group): forced on small arrays through
+CUSZP_TICKET_TILES (the size-based choice takes them only for large f64 arrays), the
+reconstructions must stay identical to the oracle's, for f32 and f64 and groups of up
+to 16 tiles, including groups cut short by the last tile.  The library reads the
+variable once, so the decompressions run in a child process per ticket size."""
 import json
 import os
 import subprocess
@@ -28,7 +28,8 @@ from cuszp_b200 import codec
 for c in json.load(open(sys.argv[2])):
     stream = torch.from_numpy(np.fromfile(c["cmp"], dtype=np.uint8)).cuda()
     dims = None if c["dim"] == 1 else tuple(c["dims"])
-    out = codec.decompress(stream, (c["n"],), torch.float64, c["eb"], c["mode"], dim=c["dim"], dims=dims)
+    dt = torch.float64 if c["dtype"] == "f64" else torch.float32
+    out = codec.decompress(stream, (c["n"],), dt, c["eb"], c["mode"], dim=c["dim"], dims=dims)
     out.cpu().numpy().tofile(c["out"])
 """
 
@@ -41,15 +42,18 @@ SHAPES = [
 MODES = ["fixed", "plain", "outlier"]
 
 
-@pytest.mark.parametrize("tiles", [3, 4])
-def test_grouped_tickets_decode_like_the_oracle(tmp_path, tiles):
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("tiles", [3, 4, 16])
+def test_grouped_tickets_decode_like_the_oracle(tmp_path, tiles, dtype):
     rng = np.random.default_rng(11)
     eb = 1e-4
     cases, want = [], []
+    npt = np.float64 if dtype == "f64" else np.float32
     for si, (dim, zyx) in enumerate(SHAPES):
         n = zyx[0] * zyx[1] * zyx[2]
         x = np.cumsum(rng.normal(0, 0.01, n)) + np.sin(np.arange(n) * 0.001)
         x[rng.integers(0, n, max(1, n // 500))] *= 300   # outliers and wide blocks
+        x = x.astype(npt)
         dims = (0, 0, 0) if dim == 1 else (zyx[2], zyx[1], zyx[0])
         for mode in MODES:
             mcode = MODES.index(mode)
@@ -57,8 +61,8 @@ def test_grouped_tickets_decode_like_the_oracle(tmp_path, tiles):
             cmp_path, out_path = tmp_path / f"{si}_{mode}.cmp", tmp_path / f"{si}_{mode}.dec"
             stream.tofile(cmp_path)
             cases.append({"cmp": str(cmp_path), "out": str(out_path), "n": n, "eb": eb, "mode": mode, "dim": dim,
-                          "dims": list(dims)})
-            want.append(O.decompress(stream, n, np.float64, eb, mcode, dim, dims))
+                          "dims": list(dims), "dtype": dtype})
+            want.append(O.decompress(stream, n, npt, eb, mcode, dim, dims))
     listing = tmp_path / "cases.json"
     listing.write_text(json.dumps(cases))
     env = dict(os.environ, CUSZP_TICKET_TILES=str(tiles))
@@ -66,5 +70,5 @@ def test_grouped_tickets_decode_like_the_oracle(tmp_path, tiles):
                        timeout=600, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     for c, exp in zip(cases, want):
-        rec = np.fromfile(c["out"], dtype=np.float64)
+        rec = np.fromfile(c["out"], dtype=npt)
         assert np.array_equal(rec.view(np.uint8), exp.view(np.uint8)), c["cmp"]
