@@ -362,7 +362,7 @@ static int fixed_threads(int, int, bool) { return N; }
 template <typename T>
 static int tma_threads_of(int dim, bool comp)
 {
-    if (comp) return TmaCfg<T, 1>::THREADS;   // the same for every dimension
+    if (comp) return dim == 1 ? TmaCfg<T, 1>::THREADS : dim == 2 ? TmaCfg<T, 2>::THREADS : TmaCfg<T, 3>::THREADS;
     return dim == 1 ? DecCfg<T, 1>::THREADS : dim == 2 ? DecCfg<T, 2>::THREADS : DecCfg<T, 3>::THREADS;
 }
 
@@ -392,10 +392,8 @@ static const Variant kVariants[] = {
     {8, 8, 4, fixed_threads<256>, false, kv<8, 8, 4>, ks<8, 8, 4>},
     {16, 8, 4, fixed_threads<512>, false, kv<16, 8, 4>, ks<16, 8, 4>},
 };
-static_assert(TmaCfg<float, 1>::THREADS == TmaCfg<float, 3>::THREADS &&
-                  TmaCfg<double, 1>::THREADS == TmaCfg<double, 3>::THREADS,
-              "TMA compress thread counts depend on the element type only");
-static_assert(TmaCfg<float, 1>::TB == 8 * 16 && TmaCfg<float, 2>::TB == 8 * 8, "TMA tiles as in variant 1");
+static_assert(TmaCfg<float, 1>::TB == 8 * 16 && TmaCfg<float, 2>::TB == 8 * 8 && TmaCfg<double, 2>::TB == 8 * 8,
+              "TMA tiles as in variant 1");
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 }  // namespace cuszp

@@ -33,7 +33,11 @@ namespace cuszp {
 
 template <typename T, int DIM>
 struct TmaCfg {
-    static constexpr int WARPS = 8;                           // codec warps
+    // codec warps x data blocks per codec warp: f64 2D/3D tiles go to four codec warps of
+    // 16 blocks (a warp's fixed per-tile costs spread over twice the blocks: 3 % faster on
+    // the 8192^2 f64 array; f32 measured slower so), everything else to eight warps
+    static constexpr bool WIDE = DIM != 1 && sizeof(T) == 8;
+    static constexpr int WARPS = WIDE ? 4 : 8;
     // tiles between packing and writing out: a tile's offset must be resolved by then
     // (the look-back takes about as long as two f32 tiles, or three f64 tiles: f64
     // tiles are load-bound and shorter)
@@ -49,7 +53,7 @@ struct TmaCfg {
     static_assert(NC % RESOLVERS == 0, "each tile state has one resolver");
     static constexpr int LOADER = WARPS;                      // warp index of the loader
     static constexpr int THREADS = 32 * (WARPS + 1 + RESOLVERS);
-    static constexpr int BPW = DIM == 1 ? 16 : 8;             // data blocks per codec warp
+    static constexpr int BPW = DIM == 1 || WIDE ? 16 : 8;     // data blocks per codec warp
     static constexpr int TB = WARPS * BPW;                    // data blocks per tile
     static constexpr int BLK = DIM == 1 ? 32 : 64;            // elements per data block
     static constexpr int TILE_ELEMS = TB * BLK;               // 4096
@@ -390,15 +394,17 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
     }
     if constexpr (DIM != 1) {
         if constexpr (MODE == MODE_OUTLIER) {
-            // element 0's bytes of every outlier block at once: lane 4j + i writes byte i of
-            // block j; the planes then start past them (myoff: block j's sign words)
-            static_assert(4 * C::BPW <= 32, "four lanes per block");
+            // element 0's bytes of every outlier block: lane 4j + i writes byte i of block j,
+            // eight blocks per step; the planes then start past them (myoff: sign words)
             const uint32_t ob = (mine & 0x80u) ? ((mine & 0x60u) >> 5) + 1u : 0u;
-            const int src = lane >> 2;
             const uint32_t i = lane & 3;
-            const uint32_t n = __shfl_sync(FULL, ob, src), v = __shfl_sync(FULL, K.o, src);
-            const uint32_t at = __shfl_sync(FULL, myoff, src);
-            if (i < n) sts_u8(out + at + i, v >> (8 * i));
+#pragma unroll
+            for (int h = 0; h < C::BPW; h += 8) {   // eight blocks per step
+                const int src = h + (lane >> 2);
+                const uint32_t n = __shfl_sync(FULL, ob, src), v = __shfl_sync(FULL, K.o, src);
+                const uint32_t at = __shfl_sync(FULL, myoff, src);
+                if (i < n) sts_u8(out + at + i, v >> (8 * i));
+            }
             myoff += ob;
         }
         const uint32_t n = MODE == MODE_OUTLIER ? (mine & 0x1fu) : mine;
