@@ -649,6 +649,19 @@ def main():
         summ[name] = _summary(r, rr)
     line["summary"] = {"peak_gbs": peak, "peak_kind": kind, "frac_unit": "of measured" if kind == "measured"
                        else "of fallback", "workloads": summ}
+    b = line.get("batched")
+    if isinstance(b, dict) and "batched_gbs" in b:
+        line["summary"]["batched"] = {"gbs": round(b["batched_gbs"], 1),
+                                      "x_plain_async": round(b["speedup_vs_plain_async"], 2),
+                                      "x_plain_sync": round(b["speedup_vs_plain_sync"], 2),
+                                      "identical": b["byte_identical_per_array"]}
+    sv = line.get("serving")
+    if isinstance(sv, dict) and "error" not in sv:
+        line["summary"]["serving"] = {
+            rate: {"gbs": round(v["batched"]["throughput_gbs"], 1), "p50_ms": round(v["batched"]["p50_ms"], 3),
+                   "p99_ms": round(v["batched"]["p99_ms"], 3), "one_at_a_time_p99_ms": round(v["one_at_a_time"]["p99_ms"], 3),
+                   "one_at_a_time_gbs": round(v["one_at_a_time"]["throughput_gbs"], 1), "identical": v["identical_results"]}
+            for rate, v in sv.items()}
     print(json.dumps(line), flush=True)
 
 
