@@ -567,6 +567,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and serving forms")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
+    ap.add_argument("--batch-only", type=int, default=0, metavar="N",
+                    help="run only the batched form, over N arrays of the batched mix (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -583,6 +585,9 @@ def main():
 
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    if args.batch_only:
+        print(json.dumps({"batched": run_batched(device, count=args.batch_only)}), flush=True)
+        return
     pg = None
     if world > 1:
         import datetime

@@ -46,11 +46,7 @@ range_partial_kernel(const BatchItem* __restrict__ items, const uint32_t* __rest
         const uint64_t lo = (c - it.chunk_start) * kRangeChunk;
         const uint64_t hi = min(n, lo + kRangeChunk);
         T mx = -INFINITY, mn = INFINITY;   // NaN-skipping
-        for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            const T v = __ldcs(in + i);
-            mx = fmax(mx, v);
-            mn = fmin(mn, v);
-        }
+        range_accumulate(in, lo, hi, threadIdx.x, blockDim.x, mx, mn);
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) {
             mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));

@@ -15,6 +15,8 @@
 
 #include "codec.cuh"
 
+#include <type_traits>
+
 namespace cuszp {
 
 // Tile shape: WARPS warps per CTA, BPW data blocks per warp (TB = WARPS*BPW per tile).
@@ -335,6 +337,54 @@ __device__ __forceinline__ void lorenzo_inverse(int32_t& d0, int32_t& d1, int la
         const int32_t b1 = __shfl_sync(FULL, wsub(wadd(E1, y1), v1), lane & ~3);
         d0 = wadd(x0, b0);
         d1 = wadd(x1, b1);
+    }
+}
+
+// --------------------------------------------------------------- value range
+
+// Running NaN-skipping extrema (fmax / fmin) of in[lo, hi) over the threads t = first,
+// first + stride, ...: scalar elements up to the first 16-byte boundary, then 16-byte
+// vector loads, four in flight per thread, then the scalar tail.  Every element is read
+// once, by streaming loads.
+template <typename T>
+__device__ __forceinline__ void range_accumulate(const T* __restrict__ in, uint64_t lo, uint64_t hi, uint64_t first,
+                                                 uint64_t stride, T& mx, T& mn)
+{
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    constexpr uint64_t PER = 16 / sizeof(T);
+    if (lo >= hi) return;
+    const uint64_t skew = ((16u - ((uintptr_t)(in + lo) & 15u)) & 15u) / sizeof(T);
+    const uint64_t head = min(hi - lo, skew);
+    for (uint64_t i = lo + first; i < lo + head; i += stride) {
+        const T v = __ldcs(in + i);
+        mx = fmax(mx, v);
+        mn = fmin(mn, v);
+    }
+    const V* body = reinterpret_cast<const V*>(in + lo + head);
+    const uint64_t nv = (hi - lo - head) / PER;
+    auto take = [&](const V& v) {
+        if constexpr (sizeof(T) == 4) {
+            mx = fmax(fmax(mx, v.x), fmax(v.y, fmax(v.z, v.w)));
+            mn = fmin(fmin(mn, v.x), fmin(v.y, fmin(v.z, v.w)));
+        } else {
+            mx = fmax(mx, fmax(v.x, v.y));
+            mn = fmin(mn, fmin(v.x, v.y));
+        }
+    };
+    uint64_t i = first;
+    for (; i + 3 * stride < nv; i += 4 * stride) {
+        const V a = __ldcs(body + i), b = __ldcs(body + i + stride), c = __ldcs(body + i + 2 * stride),
+                d = __ldcs(body + i + 3 * stride);
+        take(a);
+        take(b);
+        take(c);
+        take(d);
+    }
+    for (; i < nv; i += stride) take(__ldcs(body + i));
+    for (uint64_t k = lo + head + nv * PER + first; k < hi; k += stride) {
+        const T v = __ldcs(in + k);
+        mx = fmax(mx, v);
+        mn = fmin(mn, v);
     }
 }
 

@@ -427,11 +427,8 @@ range_kernel(const T* __restrict__ in, size_t n, T* __restrict__ partial, unsign
              T* __restrict__ result)
 {
     T mx = -INFINITY, mn = INFINITY;   // NaN-skipping running extrema
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const T v = __ldcs(in + i);
-        mx = fmax(mx, v);
-        mn = fmin(mn, v);
-    }
+    range_accumulate(in, 0, n, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x, mx,
+                     mn);
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
         mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
