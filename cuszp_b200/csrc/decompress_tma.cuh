@@ -326,6 +326,12 @@ __device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t 
                  "r"(bytes)
                  : "memory");
 }
+// Starts fetching `bytes` (a multiple of 16) from global `src` (16-byte aligned) into L2,
+// with no completion to wait for: a later bulk load of the same bytes then reads L2.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
@@ -659,6 +665,9 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
                 const bool fits = agg <= (uint32_t)(C::TB * C::MAXBLK);
                 if (!fits && lane == 0) atomicOr(err, ERR_CAPACITY);
                 const uint32_t bytes = agg && fits ? (uint32_t)(a1 - a0) : 0u;
+                // the payload's address is known before the slot is free: bring it into L2
+                // now, so that the slot's load, once the codec warps release it, reads L2
+                if (lane == 0 && bytes) bulk_prefetch_l2(cmp + a0, bytes);
                 // the slot: fill m - 1 decoded
                 if (m > 0 && !mbar_wait(&sh.freed[f], (uint32_t)(m - 1) & 1u, err)) { stop = true; break; }
                 __syncwarp();   // rates and offsets are written before lane 0 publishes the fill
