@@ -375,8 +375,10 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
         }
         narrow = __all_sync(FULL, lane >= C::BPW || (mysz != 0 && myn <= 15));
     }
-    auto decode = [&](int j, int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, bool& za, bool& zb) {
-        if (narrow) {
+    // blocks j, j + 1; `nar` is `narrow`, passed as a constant by for_pairs
+    auto decode = [&](int j, bool nar, int32_t& d0a, int32_t& d1a, int32_t& d0b, int32_t& d1b, bool& za,
+                      bool& zb) {
+        if (nar) {
             const uint32_t pa = __shfl_sync(FULL, myps, j), pb = __shfl_sync(FULL, myps, j + 1);
             const uint32_t na = __shfl_sync(FULL, myn, j), nb = __shfl_sync(FULL, myn, j + 1);
             uint32_t ma = 0, mb = 0;
@@ -396,6 +398,18 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             zb = payload_size<DIM, MODE>(rb2) == 0;
         }
     };
+    // pair(j, nar) for j = 0, 2, ..: a narrow warp runs its pairs fully unrolled, with no
+    // branch between them (measured 7-8 % faster decompress of 512^3 f32 in 2D and 3D);
+    // otherwise one pair per iteration
+    auto for_pairs = [&](auto&& pair) {
+        if (narrow) {
+#pragma unroll
+            for (int j = 0; j < C::BPW; j += 2) pair(j, true);
+        } else {
+#pragma unroll 1
+            for (int j = 0; j < C::BPW; j += 2) pair(j, false);
+        }
+    };
     if constexpr (DIRECT) {
         // the warp's kGroup whole blocks lie in one block row (or past the array)
         T* q = nullptr;
@@ -405,11 +419,10 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             q = out + row * g.dx + (uint64_t)p.x * 8 + (uint32_t)(lane & 7);
         }
         const uint64_t half = 4ull * g.dx;   // element l + 32 is four rows down
-#pragma unroll 1
-        for (int j = 0; j < C::BPW; j += 2) {
+        for_pairs([&](int j, bool nar) {
             int32_t d0a, d1a, d0b, d1b;
             bool za, zb;
-            decode(j, d0a, d1a, d0b, d1b, za, zb);
+            decode(j, nar, d0a, d1a, d0b, d1b, za, zb);
             if constexpr (MODE != MODE_FIXED) {
                 lorenzo_inverse<DIM>(d0a, d1a, lane, ll);
                 lorenzo_inverse<DIM>(d0b, d1b, lane, ll);
@@ -421,7 +434,7 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
                 qa[8] = zb ? T(0) : dequant(d0b, eb);
                 qa[8 + half] = zb ? T(0) : dequant(d1b, eb);
             }
-        }
+        });
         __syncwarp();
         if (lane == 0) mbar_arrive(&sh.freed[f]);   // done with the payload slot
         return;
@@ -491,11 +504,10 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             sts_val(obs + (j + 1) * 32 * sizeof(T), payload_size<1, MODE>(rB) ? dequant(dB, eb) : T(0));
         }
     } else {
-#pragma unroll 1
-        for (int j = 0; j < C::BPW; j += 2) {
+        for_pairs([&](int j, bool nar) {
             int32_t d0a, d1a, d0b, d1b;
             bool za, zb;
-            decode(j, d0a, d1a, d0b, d1b, za, zb);
+            decode(j, nar, d0a, d1a, d0b, d1b, za, zb);
             if constexpr (MODE != MODE_FIXED) {
                 lorenzo_inverse<DIM>(d0a, d1a, lane, ll);
                 lorenzo_inverse<DIM>(d0b, d1b, lane, ll);
@@ -505,7 +517,7 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
             sts_val(oj + 32 * sizeof(T), za ? T(0) : dequant(d1a, eb));
             sts_val(oj + 64 * sizeof(T), zb ? T(0) : dequant(d0b, eb));
             sts_val(oj + 96 * sizeof(T), zb ? T(0) : dequant(d1b, eb));
-        }
+        });
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&sh.freed[f]);   // done with the payload slot
