@@ -53,12 +53,20 @@ __device__ __forceinline__ void put32s(saddr_t a, uint32_t v)
         sts_u32(a, v);
     }
 }
-// put32s where `c` holds, without a branch on `c` (the outlier-mode byte offset's
-// residue mod 4 is uniform over a block's words, so its branch does not diverge there).
-template <int MODE>
+// put32s where `c` holds, without a branch on `c`.  Outlier mode: BYTEWISE writes the
+// word as four byte stores under one predicate, with no branch at all; otherwise the
+// offset's residue mod 4 (uniform over a block's words, so the branch does not
+// diverge) picks one word, two halves, or byte + half + byte.  Bytewise measured 8 %
+// faster on the 512^3 f32 outlier 1D compress and 3.6 % in 2D, but 1 % slower in 3D.
+template <int MODE, bool BYTEWISE = false>
 __device__ __forceinline__ void put32s_if(bool c, saddr_t a, uint32_t v)
 {
-    if constexpr (MODE == MODE_OUTLIER) {
+    if constexpr (MODE == MODE_OUTLIER && BYTEWISE) {
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %5, 0;\n\t"
+                     "@p st.shared.u8 [%0], %1;\n\t@p st.shared.u8 [%0+1], %2;\n\t"
+                     "@p st.shared.u8 [%0+2], %3;\n\t@p st.shared.u8 [%0+3], %4;\n\t}"
+                     ::"r"(a), "r"(v), "r"(v >> 8), "r"(v >> 16), "r"(v >> 24), "r"((uint32_t)c) : "memory");
+    } else if constexpr (MODE == MODE_OUTLIER) {
         const uint32_t r = a & 3u;
         if (r == 0) {
             sts_u32_if(c, a, v);
@@ -570,8 +578,8 @@ __device__ __forceinline__ void pack_quad_1d_narrow(int32_t cA, int32_t cB, int3
 {
     uint32_t x1 = slot_pair(cA, cB), x2 = slot_pair(cC, cD);
     warp_transpose32x2(x1, x2, xl);
-    put32s_if<MODE>((k1 >> pl) & 1u, p1 + o, x1);
-    put32s_if<MODE>((k2 >> pl) & 1u, p2 + o, x2);
+    put32s_if<MODE, true>((k1 >> pl) & 1u, p1 + o, x1);
+    put32s_if<MODE, true>((k2 >> pl) & 1u, p2 + o, x2);
 }
 
 // Payloads of two 2D/3D blocks of rate <= 15, sign words at pa / pb, transposes
@@ -579,8 +587,8 @@ __device__ __forceinline__ void pack_quad_1d_narrow(int32_t cA, int32_t cB, int3
 // (plane 15 = the half's signs) and stores it when that bit of the block's plane mask
 // is set (ka / kb: bits 0 .. n-1 and 15 for a block with a payload, 0 without).  In
 // outlier mode element 0's magnitude must already be cleared (sign kept) where the
-// block stores element 0 ahead of its planes.
-template <int MODE>
+// block stores element 0 ahead of its planes.  BYTEWISE: as for put32s_if.
+template <int MODE, bool BYTEWISE = false>
 __device__ __forceinline__ void pack_pair_narrow(uint32_t ka, uint32_t kb, int32_t c0a, int32_t c1a, int32_t c0b,
                                                  int32_t c1b, saddr_t pa, saddr_t pb, int lane, const XposeLane& xl)
 {
@@ -589,8 +597,8 @@ __device__ __forceinline__ void pack_pair_narrow(uint32_t ka, uint32_t kb, int32
     const uint32_t pl = (lane ^ 7) & 15;
     const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
     const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
-    put32s_if<MODE>((ka >> pl) & 1u, pa + o, xa);
-    put32s_if<MODE>((kb >> pl) & 1u, pb + o, xb);
+    put32s_if<MODE, BYTEWISE>((ka >> pl) & 1u, pa + o, xa);
+    put32s_if<MODE, BYTEWISE>((kb >> pl) & 1u, pb + o, xb);
 }
 
 // Plane mask of a block for pack_pair_narrow (rate byte r, n <= 15 planes).

@@ -422,8 +422,9 @@ __device__ __forceinline__ void pack_codes(const WarpCodes<DIM, C>& K, saddr_t o
             for (int j = 0; j < C::BPW; j += 2) {
                 const uint32_t ka = __shfl_sync(FULL, mask, j), kb = __shfl_sync(FULL, mask, j + 1);
                 const uint32_t oa = __shfl_sync(FULL, myoff, j), ob = __shfl_sync(FULL, myoff, j + 1);
-                pack_pair_narrow<MODE>(ka, kb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob, lane,
-                                       xl);
+                // byte-wise outlier stores in 2D only (3D measured 1 % slower with them)
+                pack_pair_narrow<MODE, DIM == 2>(ka, kb, K.c0[j], K.c1[j], K.c0[j + 1], K.c1[j + 1], out + oa, out + ob,
+                                                 lane, xl);
             }
             return;
         }
