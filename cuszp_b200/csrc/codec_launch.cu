@@ -197,13 +197,26 @@ static EncodeTiledFn encode_tiled()
     return fn;
 }
 
+// CUSZP_NO_ROW_BOXES=1 in the environment keeps f32 3D arrays on one box per block.
+static bool row_boxes_allowed()
+{
+    static const bool ok = [] {
+        const char* e = std::getenv("CUSZP_NO_ROW_BOXES");
+        return !(e && e[0] == '1');
+    }();
+    return ok;
+}
+
 // 2D/3D tensor map of an array for the TMA kernels.  2D arrays whose blocks are all
 // whole and whose block rows hold whole groups get a grouped map: the array as the 5D
 // tensor (column in block, row in block, block column, block row, slice), so that one
 // box of kGroup whole blocks lands in shared memory in block order (k = 8r + c per
-// block); *grouped is set then.  Otherwise the array as a 3D tensor (x fastest) with
-// one data block per box, out-of-array elements zero-filled on loads and clipped on
-// stores.
+// block); *grouped is set then.  f32 3D arrays whose rows hold whole rows of 8 blocks
+// (dx a multiple of 32) get a row-box map, *grouped set too: one 32 x 4 x 4 box is a
+// codec warp's 8 blocks, stored 128-byte swizzled (128-byte rows, so the kernels' reads
+// and writes of it are free of bank conflicts), one load or store per warp instead of
+// eight.  Otherwise the array as a 3D tensor (x fastest) with one data block per box.
+// Out-of-array elements are zero-filled on loads and clipped on stores.
 bool make_block_map(CUtensorMap* m, const Problem& p, const void* in, bool* grouped)
 {
     EncodeTiledFn enc = encode_tiled();
@@ -225,6 +238,16 @@ bool make_block_map(CUtensorMap* m, const Problem& p, const void* in, bool* grou
     }
     const cuuint64_t dims[3] = {p.g.dx, p.g.dy, p.g.dz};
     const cuuint64_t strides[2] = {p.g.dx * esz, (cuuint64_t)p.g.dx * p.g.dy * esz};
+    if (p.dim == 3 && p.type == 0 && p.g.dx % 32 == 0 && row_boxes_allowed()) {
+        const cuuint32_t rbox[3] = {32, 4, 4};
+        const cuuint32_t restr[3] = {1, 1, 1};
+        if (enc(m, dt, 3, const_cast<void*>(in), dims, strides, rbox, restr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
+            *grouped = true;
+            return true;
+        }
+    }
     const cuuint32_t box[3] = {p.dim == 2 ? 8u : 4u, p.dim == 2 ? 8u : 4u, p.dim == 2 ? 1u : 4u};
     const cuuint32_t estr[3] = {1, 1, 1};
     return enc(m, p.type == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,

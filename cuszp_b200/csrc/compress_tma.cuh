@@ -69,7 +69,10 @@ struct TmaCfg {
     static constexpr int OFF_IN = 0;
     static constexpr int OFF_STG = NIN * TILE_BYTES;
     static constexpr int BYTES = OFF_STG + WARPS * RING + 16;   // + what a copy-out may read past a ring
-    static constexpr size_t smem_bytes() { return (size_t)BYTES + 128; }   // + base alignment
+    // base alignment: 3D input slots take 128-byte swizzled boxes, whose pattern follows
+    // the shared address bits and so needs 1024-byte aligned slots
+    static constexpr unsigned ALIGN = DIM == 3 ? 1024u : 128u;
+    static constexpr size_t smem_bytes() { return (size_t)BYTES + ALIGN; }
     static_assert(TB == Tiling<DIM>::TB, "tiles must match the workspace layout");
     static_assert(DIM == 1 || TB % kGroup == 0, "tiles hold whole groups");
 };
@@ -264,21 +267,33 @@ __device__ __forceinline__ uint32_t codes_1d(saddr_t tin, WarpCodes<1, C>& K, in
     return __reduce_add_sync(FULL, payload_size<1, MODE>(K.rb));
 }
 
-// 2D/3D code phase: the warp's 8 blocks (each block's 64 elements contiguous in `tin`).
-template <typename T, int DIM, int MODE, typename C>
+// 2D/3D code phase: the warp's 8 blocks.  Lane l codes element l and l + 32 of each
+// block (element k = 8r + c in 2D, 16z + 4y + x in 3D).  In the input slot the block's
+// 64 elements are contiguous, or with SWZ (f32 3D row boxes) the warp's blocks are one
+// 32 x 4 x 4 box stored 128-byte swizzled: row r = 4z + y at 128 r bytes, block j's four
+// elements of that row in its 16-byte chunk j ^ (r & 7).  A lane's 32 first-half (and
+// 32 second-half) reads then hit 32 different banks.
+template <typename T, int DIM, int MODE, typename C, bool SWZ = false>
 __device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, int warp, int64_t t, const Geom& g,
                                              T recip, uint8_t* __restrict__ cmp, int lane)
 {
     constexpr uint32_t B = DIM == 2 ? 8 : 4;
     static_assert(C::BPW % 4 == 0, "blocks are coded four at a time");
+    static_assert(!SWZ || (DIM == 3 && sizeof(T) == 4 && C::BPW == 8), "row boxes are f32 3D, 8 blocks per warp");
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-    const saddr_t wb = tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);   // this lane's element
+    // this lane's element of block 0 (SWZ: before the chunk swizzle) and of the second half
+    const saddr_t wb = SWZ ? tin + warp * C::BPW * 64 * (uint32_t)sizeof(T) + (uint32_t)(lane >> 2) * 128u +
+                                 (uint32_t)(lane & 3) * 4u
+                           : tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);
+    const uint32_t sw = SWZ ? (uint32_t)(lane >> 2) << 4 : 0u;
+    constexpr uint32_t H1 = SWZ ? 1024u : 32u * (uint32_t)sizeof(T);
+    auto blk_at = [&](int j) -> saddr_t { return SWZ ? wb + (((uint32_t)j << 4) ^ sw) : wb + j * 64 * sizeof(T); };
     const uint32_t nblk = b0 < g.nblocks ? (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0) : 0u;
     // partial blocks exist only along axes the block size does not divide
     const bool ragged = (g.dx % B) || (g.dy % B) || (DIM == 3 && (g.dz % 4));
     auto code_pair = [&](saddr_t blk, int32_t& c0, int32_t& c1) {
         const int32_t q0 = quantize(lds_val<T>(blk), recip);
-        const int32_t q1 = quantize(lds_val<T>(blk + 32 * sizeof(T)), recip);
+        const int32_t q1 = quantize(lds_val<T>(blk + H1), recip);
         c0 = q0;
         c1 = q1;
         if constexpr (MODE != MODE_FIXED) {
@@ -291,7 +306,7 @@ __device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, 
     if (!ragged && nblk == C::BPW) {
         // every block whole: no masks, four independent blocks per step
 #pragma unroll
-        for (int j = 0; j < C::BPW; j++) code_pair(wb + j * 64 * sizeof(T), K.c0[j], K.c1[j]);
+        for (int j = 0; j < C::BPW; j++) code_pair(blk_at(j), K.c0[j], K.c1[j]);
     } else {
         // blocks past the warp's last (nblk) or elements past the array: code 0
         const BlockPos bp = block_pos(b0 < g.nblocks ? b0 : 0, g);
@@ -304,7 +319,7 @@ __device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, 
 #pragma unroll
         for (int j = 0; j < C::BPW; j++) {
             int32_t c0, c1;
-            code_pair(wb + j * 64 * sizeof(T), c0, c1);
+            code_pair(blk_at(j), c0, c1);
             const uint32_t xb = bx * B, yb = by * B, zb = DIM == 2 ? bz : bz * 4;
             const bool inx = xb + cx < g.dx;
             const bool ok0 = (uint32_t)j < nblk && inx && yb + ry0 < g.dy && (DIM == 2 || zb + rz0 < g.dz);
@@ -532,7 +547,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
 {
     using C = TmaCfg<T, DIM>;
     extern __shared__ unsigned char dsm[];
-    unsigned char* base = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
+    unsigned char* base = dsm + ((C::ALIGN - (smem_u32(dsm) & (C::ALIGN - 1u))) & (C::ALIGN - 1u));
     T* inbuf = reinterpret_cast<T*>(base + C::OFF_IN);
     uint8_t* stg = base + C::OFF_STG;
     __shared__ __align__(8) TmaShared<T, DIM> sh;
@@ -632,7 +647,15 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 }
                 __syncwarp();
                 if ((uint32_t)lane < nvalid) src.acquire_map(A.tmap);
-                if (DIM == 2 && g.grouped) {
+                if (DIM == 3 && g.grouped) {
+                    // one swizzled box per codec warp: its BPW blocks are one row of whole
+                    // blocks (nvalid is a multiple of BPW: block rows hold whole rows of them)
+                    if ((uint32_t)lane < (uint32_t)C::WARPS && (uint32_t)lane * C::BPW < nvalid) {
+                        const BlockPos p = block_pos(b0 + lane * C::BPW, g);
+                        tma_load_3d(dst + lane * C::BPW * 64, A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4),
+                                    &sh.full[s]);
+                    }
+                } else if (DIM == 2 && g.grouped) {
                     // kGroup whole blocks per box, landing in block order (nvalid is a
                     // multiple of kGroup: rows hold whole groups)
                     if ((uint32_t)lane * kGroup < nvalid) {
@@ -776,6 +799,9 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 uint32_t total;
                 if constexpr (DIM == 1)
                     total = codes_1d<T, MODE, C>(tin, K, warp, lt, g, recip, A.cmp, lane);
+                else if constexpr (DIM == 3 && sizeof(T) == 4)
+                    total = g.grouped ? codes_nd<T, DIM, MODE, C, true>(tin, K, warp, lt, g, recip, A.cmp, lane)
+                                      : codes_nd<T, DIM, MODE, C, false>(tin, K, warp, lt, g, recip, A.cmp, lane);
                 else
                     total = codes_nd<T, DIM, MODE, C>(tin, K, warp, lt, g, recip, A.cmp, lane);
                 __syncwarp();
