@@ -8,9 +8,11 @@
 //
 //   loader warp: takes tile tickets and loads each tile into an input slot with the
 //     Tensor Memory Accelerator -- one `cp.async.bulk` of the tile's contiguous
-//     elements in 1D, one `cp.async.bulk.tensor.3d` box per data block in 2D/3D (the
-//     box lands in the block's element order, OOB elements zero-filled) -- completing
-//     on an mbarrier.  It refills a slot as soon as the codec warps are done with it.
+//     elements in 1D; in 2D/3D one box of 8 whole blocks per codec warp where the
+//     array's map allows it (grouped 2D maps: block order; f32 3D row boxes: 32 x 4 x 4,
+//     128-byte swizzled), else one `cp.async.bulk.tensor.3d` box per data block in the
+//     block's element order; OOB elements zero-filled -- completing on an mbarrier.
+//     It refills a slot as soon as the codec warps are done with it.
 //   codec warps (tile k): quantize + Lorenzo delta from the input slot, block rates
 //     -> rate bytes, and sign maps + bit-planes packed into a span of the warp's
 //     staging ring; the last warp to finish posts the tile aggregate.
