@@ -601,6 +601,31 @@ __device__ __forceinline__ void pack_pair_narrow(uint32_t ka, uint32_t kb, int32
     put32s_if<MODE, BYTEWISE>((kb >> pl) & 1u, pb + o, xb);
 }
 
+// pack_pair_narrow for four blocks (masks k, codes c0 / c1, sign-word offsets p): four
+// transposes interleaved stage by stage, twice the independent work per dependent step
+// of the butterfly (measured 1.3 % faster on the 512^3 f32 3D compress, 1 % slower in 2D).
+template <int MODE, bool BYTEWISE = false>
+__device__ __forceinline__ void pack_quad_narrow(const uint32_t* k, const int32_t* c0, const int32_t* c1,
+                                                 const saddr_t* p, int lane, const XposeLane& xl)
+{
+    uint32_t x[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) x[i] = slot_pair(c0[i], c1[i]);
+#pragma unroll
+    for (int st = 0; st < 5; st++) {
+        uint32_t y[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) y[i] = __shfl_xor_sync(FULL, x[i], 16 >> st);
+#pragma unroll
+        for (int i = 0; i < 4; i++) x[i] = xl.stage(st, x[i], y[i]);
+    }
+    const uint32_t pl = (lane ^ 7) & 15;
+    const uint32_t h4 = (uint32_t)(lane >> 4) * 4;
+    const uint32_t o = pl == 15 ? h4 : 8 + 8 * pl + h4;
+#pragma unroll
+    for (int i = 0; i < 4; i++) put32s_if<MODE, BYTEWISE>((k[i] >> pl) & 1u, p[i] + o, x[i]);
+}
+
 // Plane mask of a block for pack_pair_narrow (rate byte r, n <= 15 planes).
 __device__ __forceinline__ uint32_t plane_mask(uint32_t r, uint32_t n) { return r ? ((1u << n) - 1u) | 0x8000u : 0u; }
 
