@@ -389,9 +389,10 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     const void* src = cmp;
     // the look-back chain limits once decoding is fast: tickets of kTicketTiles tiles
     // when every front warp still gets two of them (measured on 512^3 f32 3D and 8192^2 f64
-    // 2D: 4 tiles beat 1, 2, 3, 8 and 16; small arrays keep single-tile tickets)
+    // 2D: 4 tiles beat 1, 2, 3, 8 and 16), two tiles below that (2^24 f32 1D: 2 beat 1, 3
+    // and 4 by 2-9 %; a group may end short at the array's last tile)
     const uint64_t front = (uint64_t)grid * (k.threads / 32 - DecCfg<double, 1>::WARPS);   // front warps
-    int tickets = p.g.ntiles >= 2ull * kTicketTiles * front ? kTicketTiles : 1;
+    int tickets = p.g.ntiles >= 2ull * kTicketTiles * front ? kTicketTiles : 2;
     if (const int forced = ticket_tiles_override()) tickets = forced;
     void* args[] = {(void*)&map, (void*)&dst, (void*)&src, (void*)&g, p.type == 0 ? (void*)&ebf : (void*)&eb,
                     (void*)&hdr, (void*)&status, (void*)&tickets};

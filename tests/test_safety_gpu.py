@@ -100,14 +100,14 @@ def test_compress_async_capacity_reported_by_workspace_check():
 
 # --------------------------------------------------------------------------- bounded waits
 
-def _two_tile_case(offset):
-    """A 2D f32 array of exactly two tiles (8 x 16 blocks of 8 x 8), optionally 4 bytes
-    off the 16-byte grid (cp.async kernels instead of the TMA ones)."""
+def _tiles_case(offset, tiles=2):
+    """A 2D f32 array of exactly `tiles` tiles (8 x 8 blocks of 8 x 8 each), optionally 4
+    bytes off the 16-byte grid (cp.async kernels instead of the TMA ones)."""
     g = torch.Generator(device="cuda").manual_seed(11)
-    n = 64 * 128
+    n = 64 * 64 * tiles
     base = (torch.randn(n + 1, generator=g, device="cuda", dtype=torch.float64).cumsum(0) * 1e-2).float()
     x = base[offset // 4: offset // 4 + n]
-    return x, (64, 128, 1)
+    return x, (64, 64 * tiles, 1)
 
 
 def _poisoned_workspace(codec, nbytes, cap=2000):
@@ -124,7 +124,7 @@ def _poisoned_workspace(codec, nbytes, cap=2000):
 @pytest.mark.parametrize("offset", [0, 4], ids=["tma-kernels", "cp-async-kernels"])
 def test_lookback_timeout_is_reported_and_workspace_recovers(offset):
     codec = _codec()
-    x, dims = _two_tile_case(offset)
+    x, dims = _tiles_case(offset)
     lay = codec.Layout(x.numel(), 2, dims)
     wsb = codec.workspace_size(lay, x.dtype, "plain")
     ws = _poisoned_workspace(codec, wsb)
@@ -148,7 +148,9 @@ def test_lookback_timeout_is_reported_and_workspace_recovers(offset):
 @pytest.mark.parametrize("offset", [0, 4], ids=["tma-kernels", "cp-async-kernels"])
 def test_decompress_lookback_timeout_is_reported(offset):
     codec = _codec()
-    x, dims = _two_tile_case(0)
+    # four tiles: the TMA decompress takes this array in 2-tile tickets, so a ticket count
+    # that starts at 1 leaves group 0 unclaimed and group 1's look-back waiting on it
+    x, dims = _tiles_case(0, tiles=4)
     stream = codec.compress(x, 1e-3, "plain", dim=2, dims=dims)
     lay = codec.Layout(x.numel(), 2, dims)
     out_base = torch.zeros(x.numel() + 4, dtype=x.dtype, device="cuda")
