@@ -197,7 +197,7 @@ static EncodeTiledFn encode_tiled()
     return fn;
 }
 
-// CUSZP_NO_ROW_BOXES=1 in the environment keeps f32 3D arrays on one box per block.
+// CUSZP_NO_ROW_BOXES=1 in the environment keeps 3D arrays on one box per block.
 static bool row_boxes_allowed()
 {
     static const bool ok = [] {
@@ -211,11 +211,11 @@ static bool row_boxes_allowed()
 // whole and whose block rows hold whole groups get a grouped map: the array as the 5D
 // tensor (column in block, row in block, block column, block row, slice), so that one
 // box of kGroup whole blocks lands in shared memory in block order (k = 8r + c per
-// block); *grouped is set then.  f32 3D arrays whose rows hold whole rows of 8 blocks
-// (dx a multiple of 32) get a row-box map, *grouped set too: one 32 x 4 x 4 box is a
-// codec warp's 8 blocks, stored 128-byte swizzled (128-byte rows, so the kernels' reads
-// and writes of it are free of bank conflicts), one load or store per warp instead of
-// eight.  Otherwise the array as a 3D tensor (x fastest) with one data block per box.
+// block); *grouped is set then.  3D arrays whose rows hold whole row boxes (dx a
+// multiple of 32 f32 / 16 f64 elements) get a row-box map, *grouped set too: one box of
+// 128-byte rows x 4 x 4 holds 8 f32 / 4 f64 whole blocks, stored 128-byte swizzled (so
+// the kernels' reads and writes of it are free of bank conflicts), one load or store per
+// 8 / 4 blocks instead of one per block.  Otherwise the array as a 3D tensor (x fastest) with one data block per box.
 // Out-of-array elements are zero-filled on loads and clipped on stores.
 bool make_block_map(CUtensorMap* m, const Problem& p, const void* in, bool* grouped)
 {
@@ -238,8 +238,10 @@ bool make_block_map(CUtensorMap* m, const Problem& p, const void* in, bool* grou
     }
     const cuuint64_t dims[3] = {p.g.dx, p.g.dy, p.g.dz};
     const cuuint64_t strides[2] = {p.g.dx * esz, (cuuint64_t)p.g.dx * p.g.dy * esz};
-    if (p.dim == 3 && p.type == 0 && p.g.dx % 32 == 0 && row_boxes_allowed()) {
-        const cuuint32_t rbox[3] = {32, 4, 4};
+    // row boxes: 128-byte rows of 32 f32 / 16 f64 elements (8 / 4 blocks)
+    const cuuint32_t rx = p.type == 0 ? 32u : 16u;
+    if (p.dim == 3 && p.g.dx % rx == 0 && row_boxes_allowed()) {
+        const cuuint32_t rbox[3] = {rx, 4, 4};
         const cuuint32_t restr[3] = {1, 1, 1};
         if (enc(m, dt, 3, const_cast<void*>(in), dims, strides, rbox, restr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

@@ -220,6 +220,32 @@ struct TmaShared {
 
 // ------------------------------------------------------------------ codes and payloads
 
+// Row boxes: 3D arrays whose block rows hold whole boxes move as 128-byte-swizzled TMA
+// boxes of 128 / sizeof(T) / 4 x 4 x 4 elements (BPB = 8 f32 or 4 f64 blocks), 2048
+// bytes in 16 rows of 128 bytes: row r = 4z + y, and 16-byte chunk c of row r stored at
+// chunk c ^ (r & 7).  Lane l handles element x = l & 3, row l >> 2 of each block (the
+// block's second half, z + 2, is 8 rows = 1024 bytes on); at(j) is its byte offset in
+// block j of a run of boxes.  The 32 lanes of a half-block then read or write distinct
+// banks (f32) or two 8-byte words per bank (f64), the least possible.
+template <typename T>
+struct RowBox {
+    static constexpr int BPB = 128 / (4 * (int)sizeof(T));   // blocks per box
+    static constexpr int CPB = 4 * (int)sizeof(T) / 16;      // 16-byte chunks per block row
+    static constexpr int EPC = 16 / (int)sizeof(T);          // elements per chunk
+    uint32_t base;   // row start + offset inside the chunk
+    uint32_t k;      // (lane's chunk inside the block row ^ row) << 4
+    __device__ __forceinline__ explicit RowBox(int lane)
+    {
+        const uint32_t r = (uint32_t)lane >> 2, x = (uint32_t)lane & 3u;
+        base = r * 128u + (x % EPC) * (uint32_t)sizeof(T);
+        k = ((x / EPC) ^ (r & 7u)) << 4;
+    }
+    __device__ __forceinline__ uint32_t at(int j) const
+    {
+        return base + (uint32_t)(j / BPB) * 2048u + ((((uint32_t)(j % BPB) * CPB) << 4) ^ k);
+    }
+};
+
 // A codec warp's codes of one tile, kept in registers from the code phase to the
 // pack phase: lane l holds element l (1D: of each block; 2D/3D: elements l and l+32).
 template <int DIM, typename C>
@@ -269,27 +295,23 @@ __device__ __forceinline__ uint32_t codes_1d(saddr_t tin, WarpCodes<1, C>& K, in
     return __reduce_add_sync(FULL, payload_size<1, MODE>(K.rb));
 }
 
-// 2D/3D code phase: the warp's 8 blocks.  Lane l codes element l and l + 32 of each
-// block (element k = 8r + c in 2D, 16z + 4y + x in 3D).  In the input slot the block's
-// 64 elements are contiguous, or with SWZ (f32 3D row boxes) the warp's blocks are one
-// 32 x 4 x 4 box stored 128-byte swizzled: row r = 4z + y at 128 r bytes, block j's four
-// elements of that row in its 16-byte chunk j ^ (r & 7).  A lane's 32 first-half (and
-// 32 second-half) reads then hit 32 different banks.
+// 2D/3D code phase: the warp's blocks.  Lane l codes element l and l + 32 of each block
+// (element k = 8r + c in 2D, 16z + 4y + x in 3D).  In the input slot the block's 64
+// elements are contiguous, or with SWZ (3D row boxes) the warp's blocks are a run of
+// swizzled boxes (RowBox).
 template <typename T, int DIM, int MODE, typename C, bool SWZ = false>
 __device__ __forceinline__ uint32_t codes_nd(saddr_t tin, WarpCodes<DIM, C>& K, int warp, int64_t t, const Geom& g,
                                              T recip, uint8_t* __restrict__ cmp, int lane)
 {
     constexpr uint32_t B = DIM == 2 ? 8 : 4;
     static_assert(C::BPW % 4 == 0, "blocks are coded four at a time");
-    static_assert(!SWZ || (DIM == 3 && sizeof(T) == 4 && C::BPW == 8), "row boxes are f32 3D, 8 blocks per warp");
+    static_assert(!SWZ || (DIM == 3 && C::BPW % RowBox<T>::BPB == 0), "row boxes: 3D, whole boxes per warp");
     const uint64_t b0 = (uint64_t)t * C::TB + (uint64_t)warp * C::BPW;
-    // this lane's element of block 0 (SWZ: before the chunk swizzle) and of the second half
-    const saddr_t wb = SWZ ? tin + warp * C::BPW * 64 * (uint32_t)sizeof(T) + (uint32_t)(lane >> 2) * 128u +
-                                 (uint32_t)(lane & 3) * 4u
-                           : tin + (warp * C::BPW * 64 + lane) * (uint32_t)sizeof(T);
-    const uint32_t sw = SWZ ? (uint32_t)(lane >> 2) << 4 : 0u;
+    // this lane's element of block j (and of its second half, H1 bytes on)
+    const saddr_t wb = tin + (warp * C::BPW * 64 + (SWZ ? 0 : lane)) * (uint32_t)sizeof(T);
+    const RowBox<T> rbx(lane);
     constexpr uint32_t H1 = SWZ ? 1024u : 32u * (uint32_t)sizeof(T);
-    auto blk_at = [&](int j) -> saddr_t { return SWZ ? wb + (((uint32_t)j << 4) ^ sw) : wb + j * 64 * sizeof(T); };
+    auto blk_at = [&](int j) -> saddr_t { return SWZ ? wb + rbx.at(j) : wb + j * 64 * sizeof(T); };
     const uint32_t nblk = b0 < g.nblocks ? (uint32_t)min((uint64_t)C::BPW, g.nblocks - b0) : 0u;
     // partial blocks exist only along axes the block size does not divide
     const bool ragged = (g.dx % B) || (g.dy % B) || (DIM == 3 && (g.dz % 4));
@@ -665,11 +687,12 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 __syncwarp();
                 if ((uint32_t)lane < nvalid) src.acquire_map(A.tmap);
                 if (DIM == 3 && g.grouped) {
-                    // one swizzled box per codec warp: its BPW blocks are one row of whole
-                    // blocks (nvalid is a multiple of BPW: block rows hold whole rows of them)
-                    if ((uint32_t)lane < (uint32_t)C::WARPS && (uint32_t)lane * C::BPW < nvalid) {
-                        const BlockPos p = block_pos(b0 + lane * C::BPW, g);
-                        tma_load_3d(dst + lane * C::BPW * 64, A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4),
+                    // row boxes of BPB blocks (nvalid is a multiple of BPB: block rows hold
+                    // whole boxes), landing in the slot in tile order
+                    constexpr uint32_t BPB = RowBox<T>::BPB;
+                    if ((uint32_t)lane < C::TB / BPB && (uint32_t)lane * BPB < nvalid) {
+                        const BlockPos p = block_pos(b0 + lane * BPB, g);
+                        tma_load_3d(dst + lane * BPB * 64, A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4),
                                     &sh.full[s]);
                     }
                 } else if (DIM == 2 && g.grouped) {
@@ -816,7 +839,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
                 uint32_t total;
                 if constexpr (DIM == 1)
                     total = codes_1d<T, MODE, C>(tin, K, warp, lt, g, recip, A.cmp, lane);
-                else if constexpr (DIM == 3 && sizeof(T) == 4)
+                else if constexpr (DIM == 3)
                     total = g.grouped ? codes_nd<T, DIM, MODE, C, true>(tin, K, warp, lt, g, recip, A.cmp, lane)
                                       : codes_nd<T, DIM, MODE, C, false>(tin, K, warp, lt, g, recip, A.cmp, lane);
                 else

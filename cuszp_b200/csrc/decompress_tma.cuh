@@ -41,8 +41,8 @@ struct DecCfg {
     static constexpr int SLOT = (TB * MAXBLK + 48 + 127) / 128 * 128;
     static constexpr int OUTW = BPW * BLK * (int)sizeof(T);   // a codec warp's decoded elements
     static constexpr int OFF_SLOT = 0;
-    // 3D output buffers take 128-byte swizzled row boxes (f32 arrays whose rows hold whole
-    // rows of 8 blocks), whose pattern follows the shared address bits: 1024-byte aligned
+    // 3D output buffers take 128-byte swizzled row boxes (arrays whose block rows hold
+    // whole boxes), whose pattern follows the shared address bits: 1024-byte aligned
     static constexpr unsigned ALIGN = DIM == 3 ? 1024u : 128u;
     static constexpr int OFF_OUT = (FRONT * SLOT + (int)ALIGN - 1) / (int)ALIGN * (int)ALIGN;
     static constexpr int BYTES = DIRECT ? OFF_OUT : OFF_OUT + WARPS * OUTW;
@@ -341,17 +341,16 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 
 // Decodes a codec warp's blocks of the tile in payload slot f into its output buffer
 // `ob` and starts their stores (the caller waits for the previous stores first).
-// SWZ (f32 3D arrays with row boxes): the buffer holds the warp's 8 blocks as one
-// 32 x 4 x 4 box, 128-byte swizzled as the compressor's input slots are (row r = 4z + y
-// at 128 r bytes, block j's four elements of the row in 16-byte chunk j ^ (r & 7)), and
-// lane 0 stores it with one TMA store.
+// SWZ (3D arrays with row boxes): the buffer holds the warp's blocks as a run of
+// swizzled row boxes (RowBox, as the compressor's input slots), `obs` is its start, and
+// one lane per box stores it with one TMA store.
 template <typename T, int DIM, int MODE, bool DIRECT, bool SWZ, typename Src>
 __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray& A, DecShared<T, DIM>& sh, int f,
                                                  int rb, int64_t lt, saddr_t pay, T* ob, saddr_t obs,
                                                  const XposeLane& xl, bool& stored, int warp, int lane)
 {
     using C = DecCfg<T, DIM>;
-    static_assert(!SWZ || (DIM == 3 && sizeof(T) == 4 && C::BPW == 8), "row boxes are f32 3D, 8 blocks per warp");
+    static_assert(!SWZ || (DIM == 3 && C::BPW % RowBox<T>::BPB == 0), "row boxes: 3D, whole boxes per warp");
     const Geom g = *A.g;
     const T eb = src.eb_of(A);
     const LorenzoLane<DIM> ll(lane);
@@ -521,9 +520,9 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
                 lorenzo_inverse<DIM>(d0b, d1b, lane, ll);
             }
             if constexpr (SWZ) {
-                // obs: this lane's row start (before the chunk swizzle); second half 8 rows on
-                const uint32_t sw = (uint32_t)(lane >> 2) << 4;
-                const saddr_t oa = obs + (((uint32_t)j << 4) ^ sw), obb = obs + (((uint32_t)(j + 1) << 4) ^ sw);
+                // this lane's elements of blocks j and j + 1; second halves 8 rows on
+                const RowBox<T> rbx(lane);
+                const saddr_t oa = obs + rbx.at(j), obb = obs + rbx.at(j + 1);
                 sts_val(oa, za ? T(0) : dequant(d0a, eb));
                 sts_val(oa + 1024u, za ? T(0) : dequant(d1a, eb));
                 sts_val(obb, zb ? T(0) : dequant(d0b, eb));
@@ -558,12 +557,13 @@ __device__ __forceinline__ void decode_and_store(const Src& src, const TileArray
         // lane j stores block j (bulk groups are per thread: each storing lane
         // commits and later waits for its own)
         if (SWZ) {
-            // the warp's 8 blocks are one row box (the array's block rows hold whole rows
-            // of 8 blocks: all of them or none are inside the array)
-            if (lane == 0 && b0 < g.nblocks) {
-                const BlockPos p = block_pos(b0, g);
+            // lane i stores row box i of the warp (block rows hold whole boxes: each box
+            // is inside the array or past its last block)
+            constexpr uint32_t BPB = RowBox<T>::BPB;
+            if ((uint32_t)lane < C::BPW / BPB && b0 + lane * BPB < g.nblocks) {
+                const BlockPos p = block_pos(b0 + lane * BPB, g);
                 src.acquire_map(A.tmap);
-                tma_store_3d(A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob);
+                tma_store_3d(A.tmap, (int)(p.x * 4), (int)(p.y * 4), (int)(p.z * 4), ob + lane * BPB * 64);
                 bulk_commit();
                 stored = true;
             }
@@ -733,8 +733,6 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
         // ---------------------------------------------------------------- codec warps
         T* ob = obuf + warp * (C::BPW * C::BLK);
         const saddr_t obs = saddr(ob) + lane * (uint32_t)sizeof(T);   // this lane's element of block 0
-        // row boxes: this lane's row start (row lane >> 2, column lane & 3), before the swizzle
-        const saddr_t obr = saddr(ob) + (uint32_t)(lane >> 2) * 128u + (uint32_t)(lane & 3) * 4u;
         const XposeLane xl(lane);
         uint32_t parity = 0;      // bit f: phase parity of slot f's next fill
         uint32_t ended = 0;       // bit f: front warp f has no more tiles
@@ -752,10 +750,10 @@ __device__ __forceinline__ void decompress_tma_body(const Src& src, WsHeader* __
             const saddr_t pay = saddr(slots + f * C::SLOT);
             src.with_mode(A.mode, [&](auto m) {
                 constexpr int MODE = decltype(m)::value;
-                if constexpr (DIM == 3 && sizeof(T) == 4) {
-                    if (A.g->grouped)
-                        decode_and_store<T, DIM, MODE, DIRECT, true>(src, A, sh, f, (int)ph, lt, pay, ob, obr, xl,
-                                                                     stored, warp, lane);
+                if constexpr (DIM == 3) {
+                    if (A.g->grouped)   // row boxes: the buffer's start
+                        decode_and_store<T, DIM, MODE, DIRECT, true>(src, A, sh, f, (int)ph, lt, pay, ob, saddr(ob),
+                                                                     xl, stored, warp, lane);
                     else
                         decode_and_store<T, DIM, MODE, DIRECT, false>(src, A, sh, f, (int)ph, lt, pay, ob, obs, xl,
                                                                       stored, warp, lane);
