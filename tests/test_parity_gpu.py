@@ -108,9 +108,12 @@ SHAPES = [
     (3, (4, 1, 1), None),
     (3, (68, 37, 29), None),
     (3, (256, 130, 66), None),
-    # block rows of whole codec warps (dims.x % 32 == 0): f32 decompress stores one
-    # x-fastest box per warp; 40 blocks per row, so tiles span rows; ragged y and z
+    # 3D row boxes (dims.x % 32 == 0: f32 and f64; 40 blocks per row, so tiles span
+    # rows; ragged y and z)
     (3, (160, 22, 11), None),
+    # row boxes with y and z smaller than a block; f64 row boxes only (dims.x % 16 == 0)
+    (3, (64, 3, 2), None),
+    (3, (48, 5, 6), None),
 ]
 
 
