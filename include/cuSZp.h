@@ -231,7 +231,7 @@ int cuSZp_compress_noalloc(const void* d_oriData, unsigned char* d_cmpBytes, siz
                            float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type,
                            cuszp_mode_t mode, unsigned long long* d_cmpSize, cudaStream_t stream);
 
-/* Version string of this build. */
+/* Version string of the library. */
 const char* cuSZp_version(void);
 
 #ifdef __cplusplus
