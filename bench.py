@@ -524,18 +524,32 @@ def run_serving(device, rates=(1000.0, 5000.0, 20000.0, 50000.0), count=1500, se
     log-uniform, 80% f32, modes uniform, 1D/2D/3D, abs eb log-uniform [1e-5, 1e-2], 64 GiB
     budget; continuous batching against one-request-at-a-time calls."""
     import dataclasses
+    import gc
 
     import torch
     from cuszp_b200 import serve
     pools = serve.make_pools(device)
     out = {}
-    # one server for every rate: its lanes, plans and arena stay resident
+    # one server for every rate: its lanes, plans and arena stay resident.  Untimed
+    # warm-up traffic first (another seed), so each lane's batch plans exist before the
+    # timed rates: a plan's creation (first use of a kind/dtype/dim on a lane) is set-up
     srv = serve.Server(device, budget_bytes=64 << 30)
+    for wrate in (50000.0, 20000.0, 5000.0):
+        warm = serve.make_requests(400, wrate, pools, seed=seed + 1000)
+        srv.run(warm, open_loop=True)
+        for r in warm:
+            srv.release(r)
+        del warm
+    # and the one-at-a-time baseline's first calls of each kernel configuration
+    serve.serve_sequential(serve.make_requests(200, 50000.0, pools, seed=seed + 2000), open_loop=False)
+    torch.cuda.empty_cache()
     for rate in rates:
         reqs = serve.make_requests(count, rate, pools, seed=seed)
+        gc.collect()   # both loops are host-driven: no collector pause from earlier garbage
         b = srv.run(reqs, open_loop=True)
         seq_reqs = [dataclasses.replace(r, admitted=None, done=None, result=None, size=None, mem=0, off=-1)
                     for r in reqs]
+        gc.collect()
         seq = serve.serve_sequential(seq_reqs, open_loop=True)
         same = all(torch.equal(a.result.reshape(-1).view(torch.uint8), r.result.reshape(-1).view(torch.uint8))
                    for a, r in zip(reqs, seq_reqs))

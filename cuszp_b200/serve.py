@@ -26,7 +26,8 @@ from dataclasses import dataclass
 import torch
 
 from .batch import BatchItemC
-from .codec import MODES, TYPES, CuszpError, Layout, max_compressed_size
+from . import codec
+from .codec import MODES, TYPES, CuszpError, Layout, max_compressed_size, workspace_size
 from .pycuSZp import Uint3, lib
 
 _P = ctypes.c_void_p
@@ -116,12 +117,15 @@ class Arena:
 
 
 class _Lane:
-    """One stream with its resident batch plans (one per (kind, dtype, dim) group) and
-    size buffers; busy while a batch is on the GPU."""
+    """One stream with its resident batch plans (one per (kind, dtype, dim) group), a
+    resident single-array workspace and size buffers; busy while a batch is on the GPU."""
+
+    WS_BYTES = 1 << 20   # single-array workspace: arrays of up to ~131k tiles (512 MiB f32)
 
     def __init__(self, device, max_batch: int):
         self.stream = torch.cuda.Stream(device)
         self.plans: dict = {}
+        self.ws = torch.zeros(self.WS_BYTES, dtype=torch.uint8, device=device)
         self.sizes_dev = torch.zeros(max_batch, dtype=torch.int64, device=device)
         self.sizes_host = torch.zeros(max_batch, dtype=torch.int64, pin_memory=True)
         self.event = torch.cuda.Event()
@@ -136,7 +140,7 @@ class Server:
     releases each request after calling it)."""
 
     def __init__(self, device=None, budget_bytes: int = 64 << 30, slots: int = 4096, lanes: int = 8,
-                 max_batch: int = 1024):
+                 max_batch: int = 1024, direct_max: int = 2):
         self.device = torch.device(device or "cuda")
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -144,6 +148,9 @@ class Server:
         self.budget = self.arena.size
         self.slots = slots
         self.max_batch = max_batch
+        # batches of up to `direct_max` requests skip the batch plan: one single-array
+        # call each on the lane's stream (same kernels, same bytes; less host work)
+        self.direct_max = direct_max
         self.lanes = [_Lane(self.device, max_batch) for _ in range(lanes)]
         self.free_lanes = deque(self.lanes)
         self.inflight: list[_Lane] = []
@@ -199,11 +206,15 @@ class Server:
         reqs = []
         while self.admitted and len(reqs) < self.max_batch:
             reqs.append(self.admitted.popleft())
+        stream = lane.stream
+        sp = _P(stream.cuda_stream)
+        if len(reqs) <= self.direct_max and all(
+                workspace_size(r.layout, r.dtype, r.mode) <= lane.ws.numel() for r in reqs):
+            self._launch_direct(lane, reqs, sp)
+            return True
         groups: dict = {}
         for r in reqs:
             groups.setdefault((r.kind, r.dtype, r.dim), []).append(r)
-        stream = lane.stream
-        sp = _P(stream.cuda_stream)
         order, off = [], 0
         with torch.cuda.stream(stream):
             # inputs were produced on the default stream
@@ -247,6 +258,36 @@ class Server:
         self.batches += 1
         return True
 
+    def _launch_direct(self, lane: _Lane, reqs: list, sp):
+        """The lane's few requests as single-array calls (cuSZp_compress_async /
+        cuSZp_decompress_async) sharing the lane's workspace, stream-ordered."""
+        stream = lane.stream
+        ws = _P(lane.ws.data_ptr())
+        with torch.cuda.stream(stream):
+            stream.wait_stream(torch.cuda.default_stream(self.device))
+            for i, r in enumerate(reqs):
+                lay = r.layout
+                eb = ctypes.c_float(r.eb)
+                if r.kind == "compress":
+                    st = codec.lib.cuSZp_compress_async(_P(r.data.data_ptr()), _P(r.result.data_ptr()),
+                                                        r.result.numel(), lay.n, eb, lay.dim, Uint3(*lay.dims),
+                                                        TYPES[r.dtype], MODES[r.mode], ws, lane.ws.numel(),
+                                                        _P(lane.sizes_dev.data_ptr() + 8 * i), sp)
+                else:
+                    st = codec.lib.cuSZp_decompress_async(_P(r.result.data_ptr()), _P(r.data.data_ptr()), lay.n, eb,
+                                                          lay.dim, Uint3(*lay.dims), TYPES[r.dtype], MODES[r.mode],
+                                                          ws, lane.ws.numel(), sp)
+                if st:
+                    raise CuszpError(st, "serve " + r.kind)
+                self.launches += 1
+            lane.sizes_host[: len(reqs)].copy_(lane.sizes_dev[: len(reqs)], non_blocking=True)
+            lane.event.record(stream)
+        for r in reqs:
+            r.data.record_stream(stream)
+        lane.order = list(reqs)
+        self.inflight.append(lane)
+        self.batches += 1
+
     def poll(self, now_fn) -> list:
         finished = []
         still = []
@@ -284,11 +325,13 @@ class Server:
 
     # ---------------------------------------------------------------- driver
 
-    def run(self, requests: list, open_loop: bool = True, idle_sleep: float = 20e-6, consume=None) -> dict:
+    def run(self, requests: list, open_loop: bool = True, idle_sleep: float = 0.0, consume=None) -> dict:
         """Serve `requests` (sorted by arrival).  open_loop: requests become visible at
         their arrival time; otherwise all are available at t = 0.  consume(r), when
         given, is called as each request completes, after which its output memory is
-        released (the result view is then invalid)."""
+        released (the result view is then invalid).  idle_sleep: seconds slept between
+        polls of the lanes in flight (0: poll without sleeping -- an OS sleep overshoots
+        tens of microseconds, which a request's latency would carry)."""
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         t0 = time.perf_counter()
 
@@ -314,44 +357,60 @@ class Server:
             if self.launch():
                 continue
             if self.inflight:
-                time.sleep(idle_sleep)
+                if idle_sleep > 0:
+                    time.sleep(idle_sleep)
             elif blocked and not self.admitted:
                 # nothing in flight and the next request still does not fit
                 raise RuntimeError("request does not fit the memory budget (results not released?)")
             elif pending and open_loop:
-                wait = pending[0].arrival - now()
-                if wait > 0:
-                    time.sleep(min(wait, 1e-3))
+                _wait_until(pending[0].arrival, now, 1e-3)
         torch.cuda.synchronize(self.device)
         wall = now()
         return summarize(requests, wall, extra={"launches": self.launches, "batches": self.batches})
 
 
+def _wait_until(target: float, now_fn, most: float | None = None):
+    """Waits until now_fn() >= target (or for at most `most` seconds): OS sleeps while
+    more than 150 us remain, then spinning, so the wake-up does not overshoot."""
+    end = target if most is None else min(target, now_fn() + most)
+    while True:
+        left = end - now_fn()
+        if left <= 0:
+            return
+        if left > 150e-6:
+            time.sleep(left - 150e-6)
+
+
 def serve_sequential(requests: list, open_loop: bool = True) -> dict:
     """Baseline: one request at a time through the reference-compatible synchronous
-    entry points (cuSZp_compress / cuSZp_decompress), in arrival order."""
+    entry points (cuSZp_compress / cuSZp_decompress), in arrival order.  Outputs are
+    carved from one buffer allocated before the clock starts (as the batched server's
+    arena is), so the comparison measures batching, not per-request allocation."""
     from .pycuSZp import cuSZp
     api = cuSZp()
+    ordered = sorted(requests, key=lambda r: r.arrival)
+    offs, total = [], 0
+    for r in ordered:
+        offs.append(total)
+        total += Arena.rounded(Server._out_bytes(r))
+    buf = torch.empty(max(total, 16), dtype=torch.uint8, device=ordered[0].data.device) if ordered else None
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for r in sorted(requests, key=lambda r: r.arrival):
+    for r, off in zip(ordered, offs):
         if open_loop:
-            while True:
-                left = r.arrival - (time.perf_counter() - t0)
-                if left <= 0:
-                    break
-                time.sleep(min(1e-3, left))
+            _wait_until(r.arrival, lambda: time.perf_counter() - t0)
         r.admitted = time.perf_counter() - t0
         lay = r.layout
         t = TYPES[r.dtype]
         if r.kind == "compress":
-            out = torch.empty(max(16, max_compressed_size(lay, r.dtype, r.mode)), dtype=torch.uint8, device=r.data.device)
+            out = buf[off: off + max(16, max_compressed_size(lay, r.dtype, r.mode))]
             size = api.compress(_P(r.data.data_ptr()), _P(out.data_ptr()), lay.n, r.eb, dim=lay.dim, dims=lay.dims,
                                 data_type=t, mode=MODES[r.mode])
             r.size = size
             r.result = out[:size]
         else:
             shape = (r.n,) if r.dim == 1 else (r.dims[2], r.dims[1], r.dims[0])
-            out = torch.empty(shape, dtype=r.dtype, device=r.data.device)
+            out = buf[off: off + r.nbytes].view(r.dtype).view(shape)
             api.decompress(_P(out.data_ptr()), _P(r.data.data_ptr()), lay.n, r.data.numel(), r.eb, dim=lay.dim,
                            dims=lay.dims, data_type=t, mode=MODES[r.mode])
             r.result = out
