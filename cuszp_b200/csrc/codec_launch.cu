@@ -391,10 +391,13 @@ static int launch_dtma(const Problem& p, const void* cmp, void* out, double eb, 
     const void* src = cmp;
     // the look-back chain limits once decoding is fast: tickets of kTicketTiles tiles
     // when every front warp still gets two of them (measured on 512^3 f32 3D and 8192^2 f64
-    // 2D: 4 tiles beat 1, 2, 3, 8 and 16), two tiles below that (2^24 f32 1D: 2 beat 1, 3
-    // and 4 by 2-9 %; a group may end short at the array's last tile)
+    // 2D: 4 tiles beat 1, 2, 3, 8 and 16), two tiles while there are more tiles than front
+    // warps (2^23 and 2^24 f32 1D: 2 beat 1, 3 and 4 by 2-11 %; a group may end short at
+    // the array's last tile), single tiles below that: a front warp loads a group's tiles
+    // one after another into its one slot, and with fewer tiles than front warps that
+    // serialisation costs more than the shorter chain saves (2^16-2^20 f32: 1 tile 4 us faster)
     const uint64_t front = (uint64_t)grid * (k.threads / 32 - DecCfg<double, 1>::WARPS);   // front warps
-    int tickets = p.g.ntiles >= 2ull * kTicketTiles * front ? kTicketTiles : 2;
+    int tickets = p.g.ntiles >= 2ull * kTicketTiles * front ? kTicketTiles : p.g.ntiles >= front ? 2 : 1;
     if (const int forced = ticket_tiles_override()) tickets = forced;
     void* args[] = {(void*)&map, (void*)&dst, (void*)&src, (void*)&g, p.type == 0 ? (void*)&ebf : (void*)&eb,
                     (void*)&hdr, (void*)&status, (void*)&tickets};

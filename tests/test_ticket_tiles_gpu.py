@@ -1,7 +1,7 @@
 """The TMA decompress kernel's tickets (one or several consecutive tiles per ticket,
 one look-back status word per group): forced through CUSZP_TICKET_TILES (the size-based
-choice takes 4 tiles for large arrays and 2 otherwise, which every other decompress test
-runs), the reconstructions must stay identical to the oracle's, for f32 and f64, single
+choice takes 4 tiles for large arrays, 2 for arrays of more tiles than front warps and 1
+below that, which the other decompress tests run), the reconstructions must stay identical to the oracle's, for f32 and f64, single
 tiles and groups of up to 16 tiles, including groups cut short by the last tile.  The library reads the
 variable once, so the decompressions run in a child process per ticket size."""
 import json
@@ -43,7 +43,7 @@ MODES = ["fixed", "plain", "outlier"]
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
-@pytest.mark.parametrize("tiles", [1, 3, 4, 16])
+@pytest.mark.parametrize("tiles", [1, 2, 3, 4, 16])
 def test_grouped_tickets_decode_like_the_oracle(tmp_path, tiles, dtype):
     rng = np.random.default_rng(11)
     eb = 1e-4
