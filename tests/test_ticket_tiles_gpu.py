@@ -72,3 +72,35 @@ def test_grouped_tickets_decode_like_the_oracle(tmp_path, tiles, dtype):
     for c, exp in zip(cases, want):
         rec = np.fromfile(c["out"], dtype=npt)
         assert np.array_equal(rec.view(np.uint8), exp.view(np.uint8)), c["cmp"]
+
+
+@pytest.mark.parametrize("tiles", [4, 16])
+def test_multi_tile_fills_with_empty_tiles(tmp_path, tiles):
+    """1D arrays in 4-tile (or larger) tickets pack several tiles into one slot fill; runs
+    of all-zero tiles (no payload bytes) at the start, middle and end of groups must
+    decode like the oracle in every mode."""
+    rng = np.random.default_rng(5)
+    n = 300_001
+    x = np.zeros(n, dtype=np.float32)
+    for lo, hi in ((5_000, 9_000), (40_000, 41_000), (120_000, 190_000), (295_000, 300_001)):
+        x[lo:hi] = (np.cumsum(rng.normal(0, 0.01, hi - lo)) + np.sin(np.arange(hi - lo) * 0.01)).astype(np.float32)
+    x[rng.integers(0, n, 50)] *= 500   # outliers and wide blocks inside the dense runs
+    eb = 1e-4
+    cases, want = [], []
+    for mode in MODES:
+        mcode = MODES.index(mode)
+        stream, _ = O.compress(x, eb, mcode, 1, (0, 0, 0))
+        cmp_path, out_path = tmp_path / f"z_{mode}.cmp", tmp_path / f"z_{mode}.dec"
+        stream.tofile(cmp_path)
+        cases.append({"cmp": str(cmp_path), "out": str(out_path), "n": n, "eb": eb, "mode": mode, "dim": 1,
+                      "dims": [0, 0, 0], "dtype": "f32"})
+        want.append(O.decompress(stream, n, np.float32, eb, mcode, 1, (0, 0, 0)))
+    listing = tmp_path / "cases.json"
+    listing.write_text(json.dumps(cases))
+    env = dict(os.environ, CUSZP_TICKET_TILES=str(tiles))
+    r = subprocess.run([sys.executable, "-c", CHILD, ROOT, str(listing)], capture_output=True, text=True,
+                       timeout=600, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for c, exp in zip(cases, want):
+        rec = np.fromfile(c["out"], dtype=np.float32)
+        assert np.array_equal(rec.view(np.uint8), exp.view(np.uint8)), c["cmp"]
