@@ -14,6 +14,7 @@
 #include "decompress_tma.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <type_traits>
 #include <cstring>
 #include <vector>
@@ -681,6 +682,17 @@ extern "C" int cuSZp_batch_plan_check(cuszp_batch_plan_t p, cudaStream_t stream)
 {
     if (!p) return E_ARG;
     return cuSZp_workspace_check(p->d_ws, p->ws_bytes, stream);
+}
+
+extern "C" int cuSZp_batch_plan_error_async(cuszp_batch_plan_t p, unsigned int* h_err, cudaStream_t stream)
+{
+    if (!p || !h_err) return E_ARG;
+    if (!p->d_ws) {
+        *h_err = 0u;
+        return OK;
+    }
+    const char* w = static_cast<const char*>(p->d_ws) + offsetof(WsHeader, err);
+    return cudaMemcpyAsync(h_err, w, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream) == cudaSuccess ? OK : E_CUDA;
 }
 
 extern "C" int cuSZp_batch_plan_variant(cuszp_batch_plan_t p, int* variant, int* threadsPerBlock, int* tma)

@@ -38,6 +38,10 @@ lib.cuSZp_batch_plan_update.argtypes = [_P, ctypes.c_int, ctypes.POINTER(BatchIt
 lib.cuSZp_batch_plan_update.restype = ctypes.c_int
 lib.cuSZp_batch_plan_execute.argtypes = [_P, _P, _P]
 lib.cuSZp_batch_plan_execute.restype = ctypes.c_int
+lib.cuSZp_batch_plan_error_async.argtypes = [_P, _P, _P]
+lib.cuSZp_batch_plan_error_async.restype = ctypes.c_int
+lib.cuSZp_batch_plan_check.argtypes = [_P, _P]
+lib.cuSZp_batch_plan_check.restype = ctypes.c_int
 lib.cuSZp_batch_plan_destroy_async.argtypes = [_P, _P]
 lib.cuSZp_batch_plan_destroy_async.restype = None
 
@@ -126,6 +130,10 @@ class _Lane:
         self.stream = torch.cuda.Stream(device)
         self.plans: dict = {}
         self.ws = torch.zeros(self.WS_BYTES, dtype=torch.uint8, device=device)
+        # sticky error words of the batch's launches, copied back with the sizes
+        # (entry i: plan i of the batch, or the lane workspace for direct calls)
+        self.err_host = torch.zeros(64, dtype=torch.int32, pin_memory=True)
+        self.err_src: list = []   # per entry: a plan handle, or None for the lane workspace
         self.sizes_dev = torch.zeros(max_batch, dtype=torch.int64, device=device)
         self.sizes_host = torch.zeros(max_batch, dtype=torch.int64, pin_memory=True)
         self.event = torch.cuda.Event()
@@ -216,6 +224,7 @@ class Server:
         for r in reqs:
             groups.setdefault((r.kind, r.dtype, r.dim), []).append(r)
         order, off = [], 0
+        lane.err_src = []
         with torch.cuda.stream(stream):
             # inputs were produced on the default stream
             stream.wait_stream(torch.cuda.default_stream(self.device))
@@ -246,6 +255,10 @@ class Server:
                 st = lib.cuSZp_batch_plan_execute(h, _P(lane.sizes_dev.data_ptr() + 8 * off), sp)
                 if st:
                     raise CuszpError(st, "batch execute")
+                st = lib.cuSZp_batch_plan_error_async(h, _P(lane.err_host.data_ptr() + 4 * len(lane.err_src)), sp)
+                if st:
+                    raise CuszpError(st, "batch error read-back")
+                lane.err_src.append(h)
                 order.extend(rs)
                 off += len(rs)
                 self.launches += 1
@@ -281,6 +294,9 @@ class Server:
                     raise CuszpError(st, "serve " + r.kind)
                 self.launches += 1
             lane.sizes_host[: len(reqs)].copy_(lane.sizes_dev[: len(reqs)], non_blocking=True)
+            # the workspace header's error word (bytes 8-11)
+            lane.err_host[:1].copy_(lane.ws[8:12].view(torch.int32), non_blocking=True)
+            lane.err_src = [None]
             lane.event.record(stream)
         for r in reqs:
             r.data.record_stream(stream)
@@ -288,11 +304,41 @@ class Server:
         self.inflight.append(lane)
         self.batches += 1
 
+    def _raise_lane_error(self, lane: _Lane):
+        """A launch of the lane set its error word (a device wait that gave up, or a
+        stream that did not fit).  The batch's requests get no result: their memory goes
+        back to the arena and the lane back to the free list, so the server stays usable;
+        then the error is raised with the library's status, whose check also resets the
+        workspace for later calls."""
+        sp = _P(lane.stream.cuda_stream)
+        status = 0
+        for src, e in zip(lane.err_src, lane.err_host[: len(lane.err_src)].tolist()):
+            if not e:
+                continue
+            if src is None:
+                st = codec.lib.cuSZp_workspace_check(_P(lane.ws.data_ptr()), lane.ws.numel(), sp)
+            else:
+                st = lib.cuSZp_batch_plan_check(src, sp)
+            status = status or st or 4
+        failed = lane.order
+        for r in failed:
+            self.release(r)
+            r.result = None
+            self.active -= 1
+        lane.order = []
+        lane.err_src = []
+        self.inflight.remove(lane)
+        self.free_lanes.append(lane)
+        raise CuszpError(status, "serve: a batch of %d request(s) on lane %d failed"
+                         % (len(failed), self.lanes.index(lane)))
+
     def poll(self, now_fn) -> list:
         finished = []
         still = []
         for lane in self.inflight:
             if lane.event.query():
+                if lane.err_src and any(lane.err_host[: len(lane.err_src)].tolist()):
+                    self._raise_lane_error(lane)
                 t = now_fn()
                 sizes = lane.sizes_host[: len(lane.order)].tolist()
                 for i, r in enumerate(lane.order):

@@ -209,6 +209,11 @@ int cuSZp_batch_plan_variant(cuszp_batch_plan_t plan, int* variant, int* threads
 int cuSZp_batch_plan_eb(cuszp_batch_plan_t plan, float* errorBounds, cudaStream_t stream);
 /* Synchronize and report a timed-out device wait (CUSZP_ERROR_TIMEOUT). */
 int cuSZp_batch_plan_check(cuszp_batch_plan_t plan, cudaStream_t stream);
+/* No reference counterpart.  Enqueue on `stream` a copy of the plan's sticky error word
+ * (0: no error) into *h_err (pinned host memory), without synchronizing: a caller that
+ * polls for completion reads it once the stream's work is done, and calls
+ * cuSZp_batch_plan_check() only when it is non-zero. */
+int cuSZp_batch_plan_error_async(cuszp_batch_plan_t plan, unsigned int* h_err, cudaStream_t stream);
 void cuSZp_batch_plan_destroy(cuszp_batch_plan_t plan);
 /* Release a plan once the work already enqueued on `stream` is done (stream-ordered free). */
 void cuSZp_batch_plan_destroy_async(cuszp_batch_plan_t plan, cudaStream_t stream);

@@ -92,3 +92,34 @@ def test_arena_first_fit_merges_free_blocks():
     a.free(0, 2048)
     a.free(z, 1000)
     assert a.used == 0 and a.starts == [0] and a.lens == [4096]
+
+
+def test_device_wait_timeout_is_raised_and_lane_recovers():
+    """A launch whose bounded device wait gives up must not hand back a result: the lane's
+    error word comes back with the sizes and the server raises the library's status
+    (the wait is made to run out on purpose: a workspace whose ticket count starts at 1
+    leaves tile 0 unclaimed, and a wait cap of 2000 ends tile 1's look-back soon)."""
+    from cuszp_b200 import codec, serve
+    g = torch.Generator(device="cuda").manual_seed(9)
+    x = (torch.randn(3 * 4096 * 8, generator=g, device="cuda", dtype=torch.float64).cumsum(0) * 1e-2).float()
+
+    def req(rid):
+        return serve.Request(rid=rid, kind="compress", dtype=torch.float32, mode="plain", dim=1, dims=(0, 0, 0),
+                             eb=1e-3, data=x, n=x.numel(), arrival=0.0)
+
+    srv = serve.Server(budget_bytes=64 << 20, lanes=1, max_batch=4)
+    lane = srv.lanes[0]
+    hdr = lane.ws[:16].view(torch.int32)
+    hdr[0] = 1          # ticket: tile 0 is never handed out
+    hdr[3] = 2000       # wait cap
+    torch.cuda.synchronize()
+    with pytest.raises(codec.CuszpError) as ei:
+        srv.run([req(0)], open_loop=False)
+    assert ei.value.status == 4, ei.value    # CUSZP_ERROR_TIMEOUT
+    # the failed request got no result and gave its memory back; the check reset the
+    # workspace, so the same lane serves the next request normally
+    assert srv.used == 0 and srv.active == 0 and not srv.inflight
+    nxt = [req(1)]
+    srv.run(nxt, open_loop=False)
+    assert torch.equal(nxt[0].result, codec.compress(x, 1e-3, "plain"))
+    srv.close()
