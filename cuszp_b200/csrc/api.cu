@@ -5,6 +5,7 @@
 #include "../../include/cuSZp.h"
 #include "codec_launch.cuh"
 
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -227,6 +228,13 @@ extern "C" int cuSZp_workspace_check(void* d_workspace, size_t workspaceBytes, c
     }
     if (st && cudaStreamSynchronize(stream) != cudaSuccess) return E_CUDA;
     return st;
+}
+
+extern "C" int cuSZp_workspace_error_async(void* d_workspace, unsigned int* h_err, cudaStream_t stream)
+{
+    if (!d_workspace || !h_err) return E_ARG;
+    const char* w = static_cast<const char*>(d_workspace) + offsetof(WsHeader, err);
+    return cudaMemcpyAsync(h_err, w, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream) == cudaSuccess ? OK : E_CUDA;
 }
 
 extern "C" int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t cmpCapacity,

@@ -40,6 +40,8 @@ lib.cuSZp_batch_plan_execute.argtypes = [_P, _P, _P]
 lib.cuSZp_batch_plan_execute.restype = ctypes.c_int
 lib.cuSZp_batch_plan_error_async.argtypes = [_P, _P, _P]
 lib.cuSZp_batch_plan_error_async.restype = ctypes.c_int
+lib.cuSZp_workspace_error_async.argtypes = [_P, _P, _P]
+lib.cuSZp_workspace_error_async.restype = ctypes.c_int
 lib.cuSZp_batch_plan_check.argtypes = [_P, _P]
 lib.cuSZp_batch_plan_check.restype = ctypes.c_int
 lib.cuSZp_batch_plan_destroy_async.argtypes = [_P, _P]
@@ -255,13 +257,16 @@ class Server:
                 st = lib.cuSZp_batch_plan_execute(h, _P(lane.sizes_dev.data_ptr() + 8 * off), sp)
                 if st:
                     raise CuszpError(st, "batch execute")
-                st = lib.cuSZp_batch_plan_error_async(h, _P(lane.err_host.data_ptr() + 4 * len(lane.err_src)), sp)
-                if st:
-                    raise CuszpError(st, "batch error read-back")
                 lane.err_src.append(h)
                 order.extend(rs)
                 off += len(rs)
                 self.launches += 1
+            # the plans' error words after all their kernels (the words stay set until
+            # checked), so no kernel of the batch waits for a read-back
+            for i, h in enumerate(lane.err_src):
+                st = lib.cuSZp_batch_plan_error_async(h, _P(lane.err_host.data_ptr() + 4 * i), sp)
+                if st:
+                    raise CuszpError(st, "batch error read-back")
             lane.sizes_host[:off].copy_(lane.sizes_dev[:off], non_blocking=True)
             lane.event.record(stream)
         for r in reqs:
@@ -294,8 +299,10 @@ class Server:
                     raise CuszpError(st, "serve " + r.kind)
                 self.launches += 1
             lane.sizes_host[: len(reqs)].copy_(lane.sizes_dev[: len(reqs)], non_blocking=True)
-            # the workspace header's error word (bytes 8-11)
-            lane.err_host[:1].copy_(lane.ws[8:12].view(torch.int32), non_blocking=True)
+            # the lane workspace's error word
+            st = lib.cuSZp_workspace_error_async(ws, _P(lane.err_host.data_ptr()), sp)
+            if st:
+                raise CuszpError(st, "serve error read-back")
             lane.err_src = [None]
             lane.event.record(stream)
         for r in reqs:

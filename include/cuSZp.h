@@ -132,6 +132,10 @@ int cuSZp_decompress_async(void* d_decData, const unsigned char* d_cmpBytes, siz
  * device-side wait of the calls using it at that many polls / sleep slices instead
  * of the default of about two seconds; tests use it to make a wait run out fast. */
 int cuSZp_workspace_check(void* d_workspace, size_t workspaceBytes, cudaStream_t stream);
+/* No reference counterpart.  Enqueue on `stream` a copy of the workspace's sticky error
+ * word (0: no error) into *h_err (pinned host memory), without synchronizing; a caller
+ * that polls for completion calls cuSZp_workspace_check() only when it is non-zero. */
+int cuSZp_workspace_error_async(void* d_workspace, unsigned int* h_err, cudaStream_t stream);
 
 /* Synchronous forms with a status and the true stream length; workspace is taken
  * from the device's stream-ordered memory pool.  Compress writes nothing past
