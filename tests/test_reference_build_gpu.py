@@ -10,8 +10,9 @@ must be identical.  Both output buffers start zeroed: the reference leaves the
 
 Sizes: the 2^24-element f32 sinusoid field (plain, 1D) at full size, the
 uniform-with-zeros f64 field at 2048 x 2048 (fixed, 2D), the Gaussian random field
-at 128^3 (outlier, in all three processing dimensionalities), and every dtype x
-mode x dim combination on a ragged 3D shape.
+at 128^3 (outlier, in all three processing dimensionalities), every dtype x
+mode x dim combination on a ragged 3D shape, and a 4 GiB f32 array (2^30 values) in
+each processing dimensionality.
 """
 import ctypes
 import os
@@ -114,3 +115,21 @@ def test_every_combination_ragged(ref, cuda, dtype, mode, dim):
     # dims.x % 4 == 0 (the reference misreads other 2D/3D rows); y and z ragged
     x = datagen.grf_field((37, 70, 132), seed=5, device=cuda, dtype=dtype)
     _check(ref, x, 1e-3, mode, dim)
+
+
+@pytest.fixture(scope="module")
+def field_4gib(cuda):
+    """2^30 f32 values (4 GiB) as a 1024^3 array: input byte offsets reach 2^32 and the
+    streams exceed 2^31 bytes, so every offset on the path must be 64-bit."""
+    from cuszp_b200 import datagen
+    x = datagen.sinusoid_field(1 << 30, seed=7, device=cuda).reshape(1024, 1024, 1024)
+    yield x
+    del x
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dim,mode", [(1, "fixed"), (2, "plain"), (3, "outlier")])
+def test_4gib_array(ref, field_4gib, dim, mode):
+    S = _check(ref, field_4gib, 1e-3, mode, dim)
+    assert S > (1 << 29)
+    torch.cuda.empty_cache()
