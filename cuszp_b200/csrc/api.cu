@@ -237,6 +237,38 @@ extern "C" int cuSZp_workspace_error_async(void* d_workspace, unsigned int* h_er
     return cudaMemcpyAsync(h_err, w, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream) == cudaSuccess ? OK : E_CUDA;
 }
 
+extern "C" int cuSZp_serve_submit_async(int compress, const void* d_in, void* d_out, size_t outCapacity,
+                                        size_t nbEle, float errorBound, cuszp_dim_t dim, uint3 dims,
+                                        cuszp_type_t type, cuszp_mode_t mode, void* d_workspace,
+                                        size_t workspaceBytes, void* h_words, cudaStream_t producer,
+                                        cudaEvent_t order, cudaEvent_t done, cudaStream_t stream)
+{
+    if (!h_words) return E_ARG;
+    Problem p;
+    int st = make_problem(p, type, mode, dim, nbEle, dims.x, dims.y, dims.z);
+    if (st) return st;
+    // the lane's previous request is complete (its slot is free): no copy into these
+    // words is in flight, so an empty array's zero length can be written from the host
+    memset(h_words, 0, 16);
+    if (order && producer != stream) {
+        if (cudaEventRecord(order, producer) != cudaSuccess) return E_CUDA;
+        if (cudaStreamWaitEvent(stream, order, 0) != cudaSuccess) return E_CUDA;
+    }
+    st = compress ? cuSZp_compress_async(d_in, static_cast<unsigned char*>(d_out), outCapacity, nbEle, errorBound,
+                                         dim, dims, type, mode, d_workspace, workspaceBytes, nullptr, stream)
+                  : cuSZp_decompress_async(d_out, static_cast<const unsigned char*>(d_in), nbEle, errorBound, dim,
+                                           dims, type, mode, d_workspace, workspaceBytes, stream);
+    if (st) return st;
+    if (p.g.ntiles) {
+        // error word, wait cap and stream length: header bytes 8..23 in one copy
+        static_assert(offsetof(WsHeader, total) == offsetof(WsHeader, err) + 8, "err, wait_cap, total adjacent");
+        const char* w = static_cast<const char*>(d_workspace) + offsetof(WsHeader, err);
+        if (cudaMemcpyAsync(h_words, w, 16, cudaMemcpyDeviceToHost, stream) != cudaSuccess) return E_CUDA;
+    }
+    if (done && cudaEventRecord(done, stream) != cudaSuccess) return E_CUDA;
+    return OK;
+}
+
 extern "C" int cuSZp_compress_ex(const void* d_oriData, unsigned char* d_cmpBytes, size_t cmpCapacity,
                                  size_t nbEle, size_t* cmpSize, float errorBound, cuszp_dim_t dim, uint3 dims,
                                  cuszp_type_t type, cuszp_mode_t mode, cudaStream_t stream)

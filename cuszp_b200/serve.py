@@ -46,6 +46,10 @@ lib.cuSZp_batch_plan_check.argtypes = [_P, _P]
 lib.cuSZp_batch_plan_check.restype = ctypes.c_int
 lib.cuSZp_batch_plan_destroy_async.argtypes = [_P, _P]
 lib.cuSZp_batch_plan_destroy_async.restype = None
+lib.cuSZp_serve_submit_async.argtypes = [ctypes.c_int, _P, _P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_float,
+                                         ctypes.c_int, Uint3, ctypes.c_int, ctypes.c_int, _P, ctypes.c_size_t, _P,
+                                         _P, _P, _P, _P]
+lib.cuSZp_serve_submit_async.restype = ctypes.c_int
 
 
 @dataclass
@@ -128,18 +132,43 @@ class _Lane:
 
     WS_BYTES = 1 << 20   # single-array workspace: arrays of up to ~131k tiles (512 MiB f32)
 
-    def __init__(self, device, max_batch: int):
+    def __init__(self, device, max_batch: int, direct_max: int):
         self.stream = torch.cuda.Stream(device)
         self.plans: dict = {}
         self.ws = torch.zeros(self.WS_BYTES, dtype=torch.uint8, device=device)
         # sticky error words of the batch's launches, copied back with the sizes
-        # (entry i: plan i of the batch, or the lane workspace for direct calls)
+        # (entry i: plan i of the batch)
         self.err_host = torch.zeros(64, dtype=torch.int32, pin_memory=True)
-        self.err_src: list = []   # per entry: a plan handle, or None for the lane workspace
+        self.err_c = (ctypes.c_uint32 * 64).from_address(self.err_host.data_ptr())
+        self.err_src: list = []   # per entry: a plan handle
         self.sizes_dev = torch.zeros(max_batch, dtype=torch.int64, device=device)
         self.sizes_host = torch.zeros(max_batch, dtype=torch.int64, pin_memory=True)
+        self.sizes_c = (ctypes.c_int64 * max_batch).from_address(self.sizes_host.data_ptr())
+        # single-array calls: 16 pinned bytes per request (error word, stream length)
+        n = max(1, direct_max)
+        self.words = torch.zeros(2 * n, dtype=torch.int64, pin_memory=True)
+        self.words_c = (ctypes.c_uint64 * (2 * n)).from_address(self.words.data_ptr())
+        self.direct = 0           # requests of the launch in flight made as single-array calls
         self.event = torch.cuda.Event()
+        self.order_event = torch.cuda.Event()
+        # torch creates an event at its first record: do that now, so that the raw
+        # handles can go to the library
+        self.event.record(self.stream)
+        self.order_event.record(self.stream)
+        self.stream.synchronize()
         self.order: list = []
+
+    def errors(self) -> list:
+        """(source, error word) per launch of the batch in flight; source None: the lane
+        workspace."""
+        if self.direct:
+            return [(None, self.words_c[2 * i] & 0xffffffff) for i in range(self.direct)]
+        return [(h, self.err_c[i]) for i, h in enumerate(self.err_src)]
+
+    def sizes(self) -> list:
+        if self.direct:
+            return [self.words_c[2 * i + 1] for i in range(self.direct)]
+        return self.sizes_c[: len(self.order)]
 
 
 class Server:
@@ -161,7 +190,9 @@ class Server:
         # batches of up to `direct_max` requests skip the batch plan: one single-array
         # call each on the lane's stream (same kernels, same bytes; less host work)
         self.direct_max = direct_max
-        self.lanes = [_Lane(self.device, max_batch) for _ in range(lanes)]
+        self._ws_fits: dict = {}
+        self.lanes = [_Lane(self.device, max_batch, direct_max) for _ in range(lanes)]
+        self._producer = _P(torch.cuda.default_stream(self.device).cuda_stream)
         self.free_lanes = deque(self.lanes)
         self.inflight: list[_Lane] = []
         self.admitted: deque[Request] = deque()
@@ -218,10 +249,10 @@ class Server:
             reqs.append(self.admitted.popleft())
         stream = lane.stream
         sp = _P(stream.cuda_stream)
-        if len(reqs) <= self.direct_max and all(
-                workspace_size(r.layout, r.dtype, r.mode) <= lane.ws.numel() for r in reqs):
+        if len(reqs) <= self.direct_max and all(self._fits_lane_ws(r) for r in reqs):
             self._launch_direct(lane, reqs, sp)
             return True
+        lane.direct = 0
         groups: dict = {}
         for r in reqs:
             groups.setdefault((r.kind, r.dtype, r.dim), []).append(r)
@@ -276,37 +307,35 @@ class Server:
         self.batches += 1
         return True
 
+    def _fits_lane_ws(self, r: Request) -> bool:
+        """Whether r's single-array workspace fits a lane's (cached per geometry)."""
+        key = (r.n, r.dim, r.dims, r.dtype, r.mode)
+        ok = self._ws_fits.get(key)
+        if ok is None:
+            ok = self._ws_fits[key] = workspace_size(r.layout, r.dtype, r.mode) <= _Lane.WS_BYTES
+        return ok
+
     def _launch_direct(self, lane: _Lane, reqs: list, sp):
-        """The lane's few requests as single-array calls (cuSZp_compress_async /
-        cuSZp_decompress_async) sharing the lane's workspace, stream-ordered."""
-        stream = lane.stream
-        ws = _P(lane.ws.data_ptr())
-        with torch.cuda.stream(stream):
-            stream.wait_stream(torch.cuda.default_stream(self.device))
-            for i, r in enumerate(reqs):
-                lay = r.layout
-                eb = ctypes.c_float(r.eb)
-                if r.kind == "compress":
-                    st = codec.lib.cuSZp_compress_async(_P(r.data.data_ptr()), _P(r.result.data_ptr()),
-                                                        r.result.numel(), lay.n, eb, lay.dim, Uint3(*lay.dims),
-                                                        TYPES[r.dtype], MODES[r.mode], ws, lane.ws.numel(),
-                                                        _P(lane.sizes_dev.data_ptr() + 8 * i), sp)
-                else:
-                    st = codec.lib.cuSZp_decompress_async(_P(r.result.data_ptr()), _P(r.data.data_ptr()), lay.n, eb,
-                                                          lay.dim, Uint3(*lay.dims), TYPES[r.dtype], MODES[r.mode],
-                                                          ws, lane.ws.numel(), sp)
-                if st:
-                    raise CuszpError(st, "serve " + r.kind)
-                self.launches += 1
-            lane.sizes_host[: len(reqs)].copy_(lane.sizes_dev[: len(reqs)], non_blocking=True)
-            # the lane workspace's error word
-            st = lib.cuSZp_workspace_error_async(ws, _P(lane.err_host.data_ptr()), sp)
+        """The lane's few requests as single-array calls sharing the lane's workspace,
+        stream-ordered, each submitted by one library call (cuSZp_serve_submit_async:
+        the wait for the producing stream, the launch, the error word and length
+        copied back, the completion event)."""
+        ws, wsb = _P(lane.ws.data_ptr()), lane.ws.numel()
+        words = lane.words.data_ptr()
+        last = len(reqs) - 1
+        for i, r in enumerate(reqs):
+            st = lib.cuSZp_serve_submit_async(
+                r.kind == "compress", r.data.data_ptr(), r.result.data_ptr(), r.mem, r.n, r.eb, r.dim,
+                Uint3(*r.dims) if r.dim != 1 else _NO_DIMS, TYPES[r.dtype], MODES[r.mode], ws, wsb,
+                words + 16 * i, self._producer if i == 0 else None, lane.order_event.cuda_event if i == 0 else None,
+                lane.event.cuda_event if i == last else None, sp)
             if st:
-                raise CuszpError(st, "serve error read-back")
-            lane.err_src = [None]
-            lane.event.record(stream)
+                raise CuszpError(st, "serve " + r.kind)
+            self.launches += 1
+        lane.direct = len(reqs)
+        lane.err_src = []
         for r in reqs:
-            r.data.record_stream(stream)
+            r.data.record_stream(lane.stream)
         lane.order = list(reqs)
         self.inflight.append(lane)
         self.batches += 1
@@ -319,7 +348,7 @@ class Server:
         workspace for later calls."""
         sp = _P(lane.stream.cuda_stream)
         status = 0
-        for src, e in zip(lane.err_src, lane.err_host[: len(lane.err_src)].tolist()):
+        for src, e in lane.errors():
             if not e:
                 continue
             if src is None:
@@ -334,6 +363,7 @@ class Server:
             self.active -= 1
         lane.order = []
         lane.err_src = []
+        lane.direct = 0
         self.inflight.remove(lane)
         self.free_lanes.append(lane)
         raise CuszpError(status, "serve: a batch of %d request(s) on lane %d failed"
@@ -344,10 +374,10 @@ class Server:
         still = []
         for lane in self.inflight:
             if lane.event.query():
-                if lane.err_src and any(lane.err_host[: len(lane.err_src)].tolist()):
+                if any(e for _, e in lane.errors()):
                     self._raise_lane_error(lane)
                 t = now_fn()
-                sizes = lane.sizes_host[: len(lane.order)].tolist()
+                sizes = lane.sizes()
                 for i, r in enumerate(lane.order):
                     if r.kind == "compress":
                         r.size = int(sizes[i])
@@ -420,6 +450,9 @@ class Server:
         torch.cuda.synchronize(self.device)
         wall = now()
         return summarize(requests, wall, extra={"launches": self.launches, "batches": self.batches})
+
+
+_NO_DIMS = Uint3(0, 0, 0)
 
 
 def _wait_until(target: float, now_fn, most: float | None = None):

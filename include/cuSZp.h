@@ -136,6 +136,20 @@ int cuSZp_workspace_check(void* d_workspace, size_t workspaceBytes, cudaStream_t
  * word (0: no error) into *h_err (pinned host memory), without synchronizing; a caller
  * that polls for completion calls cuSZp_workspace_check() only when it is non-zero. */
 int cuSZp_workspace_error_async(void* d_workspace, unsigned int* h_err, cudaStream_t stream);
+/* No reference counterpart: one request of a serving lane in one host call.  `stream`
+ * first waits for the work queued so far on `producer` (through `order`, recorded here;
+ * skipped when `order` is NULL or producer == stream).  Then it runs
+ * cuSZp_compress_async (compress != 0; d_in values, d_out stream of outCapacity bytes)
+ * or cuSZp_decompress_async (d_in stream, d_out values) with the workspace.  Next it
+ * copies the workspace's error word and stream length into the 16 pinned host bytes
+ * at h_words: bytes 0-3 hold the error word, bytes 8-15 the compressed length.  Last,
+ * it records `done` on `stream` (skipped when NULL).  h_words must not be the target
+ * of a copy still in flight: the call zeroes it from the host first, which leaves an
+ * empty array's length 0. */
+int cuSZp_serve_submit_async(int compress, const void* d_in, void* d_out, size_t outCapacity, size_t nbEle,
+                             float errorBound, cuszp_dim_t dim, uint3 dims, cuszp_type_t type, cuszp_mode_t mode,
+                             void* d_workspace, size_t workspaceBytes, void* h_words, cudaStream_t producer,
+                             cudaEvent_t order, cudaEvent_t done, cudaStream_t stream);
 
 /* Synchronous forms with a status and the true stream length; workspace is taken
  * from the device's stream-ordered memory pool.  Compress writes nothing past

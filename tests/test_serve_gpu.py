@@ -123,3 +123,52 @@ def test_device_wait_timeout_is_raised_and_lane_recovers():
     srv.run(nxt, open_loop=False)
     assert torch.equal(nxt[0].result, codec.compress(x, 1e-3, "plain"))
     srv.close()
+
+
+def test_serve_submit_matches_single_array_calls():
+    """cuSZp_serve_submit_async: the length and error word land in the pinned words, the
+    stream and the reconstruction equal the library's own calls, the lane stream waits for
+    the producing stream, and an empty array reports length 0 with no launch."""
+    import ctypes
+    from cuszp_b200 import codec, serve  # noqa: F401  (serve declares the call's argument types)
+    from cuszp_b200.pycuSZp import Uint3, lib
+    P = ctypes.c_void_p
+    x = torch.randn(37, 70, 132, device="cuda").cumsum(2) * 1e-2
+    lay = codec.Layout.of(x, 3)
+    cap = codec.max_compressed_size(lay, x.dtype, "outlier")
+    ws = torch.zeros(1 << 20, dtype=torch.uint8, device="cuda")
+    words = torch.full((4,), -1, dtype=torch.int64, pin_memory=True)
+    lane = torch.cuda.Stream()
+    done, order = torch.cuda.Event(), torch.cuda.Event()
+    done.record(lane)
+    order.record(lane)
+    torch.cuda.synchronize()
+    out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    src = torch.zeros_like(x)
+    torch.cuda._sleep(20_000_000)   # the producer is still busy when the lane launches
+    src.copy_(x)
+    prod = P(torch.cuda.current_stream().cuda_stream)
+    st = lib.cuSZp_serve_submit_async(1, src.data_ptr(), out.data_ptr(), cap, lay.n, 1e-3, 3, Uint3(*lay.dims), 0,
+                                      2, ws.data_ptr(), ws.numel(), words.data_ptr(), prod, order.cuda_event,
+                                      done.cuda_event, P(lane.cuda_stream))
+    assert st == 0
+    done.synchronize()
+    S = int(words[1])
+    assert int(words[0]) & 0xffffffff == 0
+    ref = codec.compress(x, 1e-3, "outlier", dim=3)
+    assert S == ref.numel() and torch.equal(out[:S], ref)
+    rec = torch.zeros_like(x)
+    st = lib.cuSZp_serve_submit_async(0, out.data_ptr(), rec.data_ptr(), 0, lay.n, 1e-3, 3, Uint3(*lay.dims), 0, 2,
+                                      ws.data_ptr(), ws.numel(), words.data_ptr() + 16, None, None,
+                                      done.cuda_event, P(lane.cuda_stream))
+    assert st == 0
+    done.synchronize()
+    assert int(words[2]) & 0xffffffff == 0
+    assert torch.equal(rec, codec.decompress(ref, x.shape, x.dtype, 1e-3, "outlier", dim=3))
+    words.fill_(-1)
+    st = lib.cuSZp_serve_submit_async(1, src.data_ptr(), out.data_ptr(), cap, 0, 1e-3, 1, Uint3(0, 0, 0), 0, 2,
+                                      ws.data_ptr(), ws.numel(), words.data_ptr(), None, None, done.cuda_event,
+                                      P(lane.cuda_stream))
+    assert st == 0
+    done.synchronize()
+    assert int(words[0]) == 0 and int(words[1]) == 0
