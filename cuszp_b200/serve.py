@@ -2,23 +2,26 @@
 
 Requests of mixed size, dtype, mode and dimensionality arrive over time.  Each loop
 iteration
-  1. retires finished batches (CUDA events), hands their results out;
+  1. retires finished work (CUDA events) and hands its results out;
   2. admits arrived requests while the device-memory budget and the slot limit allow;
-  3. launches what was admitted as ONE persistent batched launch per (kind, dtype, dim)
-     group on the next free lane, so batches formed while others are still on the GPU
-     overlap with them on the device.
-State stays resident across batches: every lane keeps one batch plan per group
-(re-targeted with cuSZp_batch_plan_update: device tables and workspace are reused,
-uploads go through pinned staging memory) and its size buffers, and request outputs
-are carved out of one device arena of the budget's size, so the loop allocates no
-device memory and never synchronizes the device.  A request's result is
-byte-identical whether it runs alone or in any mix, because each array keeps its own
-look-back chain inside the batched kernel (cuszp_b200/csrc/batch.cu).
+  3. launches what was admitted on the next free lane (a stream), so work formed while
+     other lanes are on the GPU overlaps with them on the device.  Many small requests
+     go out as ONE persistent batched launch per (kind, dtype, dim) group; otherwise
+     the lane takes the queued requests as single-array calls, one native submission
+     each, and hands each result out as soon as its own call completes.
+State stays resident: every lane keeps one batch plan per group (re-targeted with
+cuSZp_batch_plan_update: device tables and workspace are reused, uploads go through
+pinned staging memory), a single-array workspace and its size and error words, and
+request outputs are carved out of one device arena of the budget's size, so the loop
+allocates no device memory and never synchronizes the device.  A request's result is
+byte-identical whichever way it runs and whatever runs beside it, because each array
+keeps its own look-back chain inside the batched kernel (cuszp_b200/csrc/batch.cu).
 """
 from __future__ import annotations
 
 import bisect
 import ctypes
+import itertools
 import time
 from collections import deque
 from dataclasses import dataclass
@@ -70,6 +73,7 @@ class Request:
     size: int | None = None
     mem: int = 0              # arena bytes held (output buffer)
     off: int = -1             # arena offset of the output buffer
+    small: bool = False       # input below the server's batch_below (set at admission)
 
     @property
     def nbytes(self) -> int:
@@ -149,12 +153,14 @@ class _Lane:
         self.words = torch.zeros(2 * n, dtype=torch.int64, pin_memory=True)
         self.words_c = (ctypes.c_uint64 * (2 * n)).from_address(self.words.data_ptr())
         self.direct = 0           # requests of the launch in flight made as single-array calls
+        self.next = 0             # ... of which the first `next` have been handed out
         self.event = torch.cuda.Event()
         self.order_event = torch.cuda.Event()
+        self.done = [torch.cuda.Event() for _ in range(n)]   # per single-array call
         # torch creates an event at its first record: do that now, so that the raw
         # handles can go to the library
-        self.event.record(self.stream)
-        self.order_event.record(self.stream)
+        for e in [self.event, self.order_event] + self.done:
+            e.record(self.stream)
         self.stream.synchronize()
         self.order: list = []
 
@@ -162,12 +168,10 @@ class _Lane:
         """(source, error word) per launch of the batch in flight; source None: the lane
         workspace."""
         if self.direct:
-            return [(None, self.words_c[2 * i] & 0xffffffff) for i in range(self.direct)]
+            return [(None, self.words_c[2 * self.next] & 0xffffffff)]
         return [(h, self.err_c[i]) for i, h in enumerate(self.err_src)]
 
     def sizes(self) -> list:
-        if self.direct:
-            return [self.words_c[2 * i + 1] for i in range(self.direct)]
         return self.sizes_c[: len(self.order)]
 
 
@@ -179,7 +183,7 @@ class Server:
     releases each request after calling it)."""
 
     def __init__(self, device=None, budget_bytes: int = 64 << 30, slots: int = 4096, lanes: int = 8,
-                 max_batch: int = 1024, direct_max: int = 2):
+                 max_batch: int = 1024, direct_max: int = 16, batch_min: int = 32, batch_below: int = 64 << 10):
         self.device = torch.device(device or "cuda")
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -187,18 +191,25 @@ class Server:
         self.budget = self.arena.size
         self.slots = slots
         self.max_batch = max_batch
-        # batches of up to `direct_max` requests skip the batch plan: one single-array
-        # call each on the lane's stream (same kernels, same bytes; less host work)
-        self.direct_max = direct_max
+        # Launch policy.  When at least `batch_min` of the admitted requests are small
+        # (input below `batch_below` bytes), those go out as one batched launch per
+        # (kind, dtype, dim) group.  Otherwise the lane takes up to `direct_max`
+        # requests as single-array calls (same kernels, same bytes), each handed out
+        # as soon as its own call completes.
+        self.direct_max = max(1, direct_max)
+        self.batch_min = batch_min
+        self.batch_below = batch_below
         self._ws_fits: dict = {}
-        self.lanes = [_Lane(self.device, max_batch, direct_max) for _ in range(lanes)]
+        self.lanes = [_Lane(self.device, max_batch, self.direct_max) for _ in range(lanes)]
         self._producer = _P(torch.cuda.default_stream(self.device).cuda_stream)
         self.free_lanes = deque(self.lanes)
         self.inflight: list[_Lane] = []
         self.admitted: deque[Request] = deque()
+        self.n_small = 0   # admitted requests marked small
         self.active = 0
         self.launches = 0
         self.batches = 0
+        self.direct_calls = 0   # requests served by single-array calls
 
     @property
     def used(self) -> int:
@@ -237,6 +248,8 @@ class Server:
         else:
             shape = (r.n,) if r.dim == 1 else (r.dims[2], r.dims[1], r.dims[0])
             r.result = view.view(r.dtype).view(shape)
+        r.small = self._in_bytes(r) < self.batch_below
+        self.n_small += r.small
         self.admitted.append(r)
         return True
 
@@ -244,14 +257,28 @@ class Server:
         if not self.admitted or not self.free_lanes:
             return False
         lane = self.free_lanes.popleft()
-        reqs = []
-        while self.admitted and len(reqs) < self.max_batch:
-            reqs.append(self.admitted.popleft())
         stream = lane.stream
         sp = _P(stream.cuda_stream)
-        if len(reqs) <= self.direct_max and all(self._fits_lane_ws(r) for r in reqs):
+        adm = self.admitted
+        small = []
+        if self.n_small >= self.batch_min:
+            small = [r for r in itertools.islice(adm, self.max_batch) if r.small]
+        if len(small) >= self.batch_min:
+            picked = set(map(id, small))
+            self.admitted = deque(r for r in adm if id(r) not in picked)
+            self.n_small -= len(small)
+            reqs = small
+        elif self._fits_lane_ws(adm[0]):
+            reqs = []
+            while adm and len(reqs) < min(self.direct_max, self.max_batch) and self._fits_lane_ws(adm[0]):
+                r = adm.popleft()
+                self.n_small -= r.small
+                reqs.append(r)
             self._launch_direct(lane, reqs, sp)
             return True
+        else:
+            reqs = [adm.popleft()]   # beyond the lane workspace: a batch of one (a plan has its own)
+            self.n_small -= reqs[0].small
         lane.direct = 0
         groups: dict = {}
         for r in reqs:
@@ -307,6 +334,10 @@ class Server:
         self.batches += 1
         return True
 
+    @staticmethod
+    def _in_bytes(r: Request) -> int:
+        return r.nbytes if r.kind == "compress" else r.data.numel()
+
     def _fits_lane_ws(self, r: Request) -> bool:
         """Whether r's single-array workspace fits a lane's (cached per geometry)."""
         key = (r.n, r.dim, r.dims, r.dtype, r.mode)
@@ -316,23 +347,24 @@ class Server:
         return ok
 
     def _launch_direct(self, lane: _Lane, reqs: list, sp):
-        """The lane's few requests as single-array calls sharing the lane's workspace,
-        stream-ordered, each submitted by one library call (cuSZp_serve_submit_async:
-        the wait for the producing stream, the launch, the error word and length
-        copied back, the completion event)."""
+        """Requests as single-array calls sharing the lane's workspace, stream-ordered,
+        each submitted by one library call (cuSZp_serve_submit_async: the wait for the
+        producing stream, the launch, the error word and length copied back, the
+        request's own completion event)."""
         ws, wsb = _P(lane.ws.data_ptr()), lane.ws.numel()
         words = lane.words.data_ptr()
-        last = len(reqs) - 1
         for i, r in enumerate(reqs):
             st = lib.cuSZp_serve_submit_async(
                 r.kind == "compress", r.data.data_ptr(), r.result.data_ptr(), r.mem, r.n, r.eb, r.dim,
                 Uint3(*r.dims) if r.dim != 1 else _NO_DIMS, TYPES[r.dtype], MODES[r.mode], ws, wsb,
                 words + 16 * i, self._producer if i == 0 else None, lane.order_event.cuda_event if i == 0 else None,
-                lane.event.cuda_event if i == last else None, sp)
+                lane.done[i].cuda_event, sp)
             if st:
                 raise CuszpError(st, "serve " + r.kind)
             self.launches += 1
+        self.direct_calls += len(reqs)
         lane.direct = len(reqs)
+        lane.next = 0
         lane.err_src = []
         for r in reqs:
             r.data.record_stream(lane.stream)
@@ -342,11 +374,14 @@ class Server:
 
     def _raise_lane_error(self, lane: _Lane):
         """A launch of the lane set its error word (a device wait that gave up, or a
-        stream that did not fit).  The batch's requests get no result: their memory goes
-        back to the arena and the lane back to the free list, so the server stays usable;
-        then the error is raised with the library's status, whose check also resets the
-        workspace for later calls."""
+        stream that did not fit).  The batch's requests not yet handed out get no
+        result: their memory goes back to the arena (once the lane's stream is idle) and
+        the lane back to the free list, so the server stays usable; then the error is
+        raised with the library's status, whose check also resets the workspace for
+        later calls.  (The error word is sticky: single-array calls after the failing
+        one on the lane fail with it.)"""
         sp = _P(lane.stream.cuda_stream)
+        lane.stream.synchronize()
         status = 0
         for src, e in lane.errors():
             if not e:
@@ -356,7 +391,7 @@ class Server:
             else:
                 st = lib.cuSZp_batch_plan_check(src, sp)
             status = status or st or 4
-        failed = lane.order
+        failed = lane.order[lane.next:] if lane.direct else lane.order
         for r in failed:
             self.release(r)
             r.result = None
@@ -369,31 +404,48 @@ class Server:
         raise CuszpError(status, "serve: a batch of %d request(s) on lane %d failed"
                          % (len(failed), self.lanes.index(lane)))
 
+    def _finish(self, r: Request, size: int, t: float, finished: list):
+        if r.kind == "compress":
+            r.size = int(size)
+            r.result = r.result[: r.size]
+            # the unused tail of the worst-case buffer goes back to the arena
+            keep = Arena.rounded(r.size)
+            if keep < r.mem:
+                self.arena.free(r.off + keep, r.mem - keep)
+                r.mem = keep
+        r.done = t
+        self.active -= 1
+        finished.append(r)
+
     def poll(self, now_fn) -> list:
         finished = []
         still = []
         for lane in self.inflight:
-            if lane.event.query():
+            if lane.direct:
+                # single-array calls complete in stream order: hand each out as its own
+                # event fires
+                w = lane.words_c
+                while lane.next < lane.direct and lane.done[lane.next].query():
+                    i = lane.next
+                    if w[2 * i] & 0xffffffff:
+                        self._raise_lane_error(lane)
+                    self._finish(lane.order[i], w[2 * i + 1], now_fn(), finished)
+                    lane.next += 1
+                if lane.next < lane.direct:
+                    still.append(lane)
+                    continue
+            elif lane.event.query():
                 if any(e for _, e in lane.errors()):
                     self._raise_lane_error(lane)
                 t = now_fn()
-                sizes = lane.sizes()
-                for i, r in enumerate(lane.order):
-                    if r.kind == "compress":
-                        r.size = int(sizes[i])
-                        r.result = r.result[: r.size]
-                        # the unused tail of the worst-case buffer goes back to the arena
-                        keep = Arena.rounded(r.size)
-                        if keep < r.mem:
-                            self.arena.free(r.off + keep, r.mem - keep)
-                            r.mem = keep
-                    r.done = t
-                    self.active -= 1
-                    finished.append(r)
-                lane.order = []
-                self.free_lanes.append(lane)
+                for r, size in zip(lane.order, lane.sizes()):
+                    self._finish(r, size, t, finished)
             else:
                 still.append(lane)
+                continue
+            lane.order = []
+            lane.direct = 0
+            self.free_lanes.append(lane)
         self.inflight = still
         return finished
 
@@ -449,7 +501,8 @@ class Server:
                 _wait_until(pending[0].arrival, now, 1e-3)
         torch.cuda.synchronize(self.device)
         wall = now()
-        return summarize(requests, wall, extra={"launches": self.launches, "batches": self.batches})
+        return summarize(requests, wall, extra={"launches": self.launches, "batches": self.batches,
+                                                "direct_calls": self.direct_calls})
 
 
 _NO_DIMS = Uint3(0, 0, 0)

@@ -16,20 +16,26 @@ def _alone(r):
                             dims=r.layout.dims if r.dim != 1 else None)
 
 
-def test_mixed_requests_identical_alone_and_in_the_mix():
+@pytest.mark.parametrize("policy", [
+    {},                                          # the defaults: single-array calls here
+    {"batch_min": 3, "batch_below": 512 << 10},  # small requests batched, the rest single
+])
+def test_mixed_requests_identical_alone_and_in_the_mix(policy):
     from cuszp_b200 import serve
     pools = serve.make_pools(torch.device("cuda"), max_bytes=8 << 20)
     reqs = serve.make_requests(120, rate=20000.0, pools=pools, seed=7, max_bytes=8 << 20, stream_pool=12)
     # a tight budget forces admission to wait for memory to free up: each result is
     # copied out as it completes and its arena memory released
-    srv = serve.Server(budget_bytes=48 << 20, lanes=3, max_batch=16)
+    srv = serve.Server(budget_bytes=48 << 20, lanes=3, max_batch=16, **policy)
 
     def consume(r):
         r.result = r.result.clone()
 
     stats = srv.run(reqs, open_loop=True, consume=consume)
     assert stats["requests"] == 120 and srv.active == 0 and srv.used == 0
-    assert srv.batches > 1
+    assert srv.batches > 1 and srv.direct_calls > 0
+    if policy:
+        assert srv.direct_calls < 120 and any(lane.plans for lane in srv.lanes)
     kinds = {r.kind for r in reqs}
     assert kinds == {"compress", "decompress"}
     assert len({(r.dtype, r.dim, r.mode) for r in reqs}) > 6
@@ -66,7 +72,8 @@ def test_resident_plans_are_reused_across_batches():
     from cuszp_b200 import serve
     pools = serve.make_pools(torch.device("cuda"), max_bytes=2 << 20)
     reqs = serve.make_requests(80, rate=0.0, pools=pools, seed=11, max_bytes=2 << 20, stream_pool=8)
-    srv = serve.Server(budget_bytes=512 << 20, lanes=2, max_batch=4)
+    # every request counts as small and three make a batch: batch plans throughout
+    srv = serve.Server(budget_bytes=512 << 20, lanes=2, max_batch=4, batch_min=3, batch_below=1 << 62)
     srv.run(reqs, open_loop=False)
     plans = sum(len(lane.plans) for lane in srv.lanes)
     assert srv.batches >= 20 and plans <= 2 * 18
