@@ -20,7 +20,9 @@ keeps its own look-back chain inside the batched kernel (cuszp_b200/csrc/batch.c
 from __future__ import annotations
 
 import bisect
+import contextlib
 import ctypes
+import gc
 import itertools
 import time
 from collections import deque
@@ -85,8 +87,12 @@ class Request:
 
 
 class Arena:
-    """First-fit allocator over one device buffer (256-byte aligned blocks, adjacent free
-    blocks merged), so serving allocates no device memory per request."""
+    """Best-fit allocator over one device buffer (256-byte aligned blocks, adjacent free
+    blocks merged), so serving allocates no device memory per request.  The free blocks
+    are kept twice, sorted by offset (for merging) and by (length, offset) (for the
+    fit), so an allocation costs a binary search however fragmented the arena is:
+    compress results give the unused tail of their worst-case buffer back, which leaves
+    many small holes."""
 
     ALIGN = 256
 
@@ -95,21 +101,28 @@ class Arena:
         self.buf = torch.empty(self.size, dtype=torch.uint8, device=device)
         self.starts = [0]            # free blocks, sorted by offset
         self.lens = [self.size]
+        self.by_size = [(self.size, 0)]   # the same blocks, sorted by (length, offset)
         self.used = 0
 
     def alloc(self, n: int) -> int:
         n = max(self.ALIGN, (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN)
-        for i, ln in enumerate(self.lens):
-            if ln >= n:
-                off = self.starts[i]
-                if ln == n:
-                    del self.starts[i], self.lens[i]
-                else:
-                    self.starts[i] += n
-                    self.lens[i] -= n
-                self.used += n
-                return off
-        return -1
+        k = bisect.bisect_left(self.by_size, (n, -1))
+        if k == len(self.by_size):
+            return -1
+        ln, off = self.by_size.pop(k)
+        i = bisect.bisect_left(self.starts, off)
+        if ln == n:
+            del self.starts[i], self.lens[i]
+        else:
+            self.starts[i] += n
+            self.lens[i] -= n
+            bisect.insort(self.by_size, (ln - n, off + n))
+        self.used += n
+        return off
+
+    def _drop(self, i: int):
+        """Removes free block i (offset order) from the size index."""
+        del self.by_size[bisect.bisect_left(self.by_size, (self.lens[i], self.starts[i]))]
 
     def free(self, off: int, n: int):
         n = max(self.ALIGN, (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN)
@@ -117,13 +130,16 @@ class Arena:
         i = bisect.bisect_left(self.starts, off)
         if i > 0 and self.starts[i - 1] + self.lens[i - 1] == off:        # merge with the block before
             i -= 1
+            self._drop(i)
             self.lens[i] += n
         else:
             self.starts.insert(i, off)
             self.lens.insert(i, n)
         if i + 1 < len(self.starts) and self.starts[i] + self.lens[i] == self.starts[i + 1]:   # and after
+            self._drop(i + 1)
             self.lens[i] += self.lens[i + 1]
             del self.starts[i + 1], self.lens[i + 1]
+        bisect.insort(self.by_size, (self.lens[i], self.starts[i]))
 
     @staticmethod
     def rounded(n: int) -> int:
@@ -199,7 +215,8 @@ class Server:
         self.direct_max = max(1, direct_max)
         self.batch_min = batch_min
         self.batch_below = batch_below
-        self._ws_fits: dict = {}
+        self._ws_fits: dict = {}   # per request geometry: fits the lane workspace
+        self._need: dict = {}      # per request geometry: output bytes
         self.lanes = [_Lane(self.device, max_batch, self.direct_max) for _ in range(lanes)]
         self._producer = _P(torch.cuda.default_stream(self.device).cuda_stream)
         self.free_lanes = deque(self.lanes)
@@ -235,7 +252,12 @@ class Server:
     def admit(self, r: Request, now: float) -> bool:
         if self.active >= self.slots:
             return False
-        need = self._out_bytes(r)
+        key = (r.kind, r.n, r.dim, r.dims, r.dtype, r.mode)
+        need = self._need.get(key)
+        if need is None:
+            if len(self._need) > 4096:
+                self._need.clear()
+            need = self._need[key] = self._out_bytes(r)
         off = self.arena.alloc(need)
         if off < 0:
             return False
@@ -343,6 +365,8 @@ class Server:
         key = (r.n, r.dim, r.dims, r.dtype, r.mode)
         ok = self._ws_fits.get(key)
         if ok is None:
+            if len(self._ws_fits) > 4096:
+                self._ws_fits.clear()
             ok = self._ws_fits[key] = workspace_size(r.layout, r.dtype, r.mode) <= _Lane.WS_BYTES
         return ok
 
@@ -467,6 +491,10 @@ class Server:
         released (the result view is then invalid).  idle_sleep: seconds slept between
         polls of the lanes in flight (0: poll without sleeping -- an OS sleep overshoots
         tens of microseconds, which a request's latency would carry)."""
+        with _gc_paused():
+            return self._run(requests, open_loop, idle_sleep, consume)
+
+    def _run(self, requests: list, open_loop: bool, idle_sleep: float, consume) -> dict:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         t0 = time.perf_counter()
 
@@ -520,11 +548,31 @@ def _wait_until(target: float, now_fn, most: float | None = None):
             time.sleep(left - 150e-6)
 
 
+@contextlib.contextmanager
+def _gc_paused():
+    """Keeps Python's cyclic garbage collector off while a loop serves; reference-counted
+    garbage is still freed at once.  A full collection pauses the host for milliseconds,
+    and every request queued behind the pause would carry it.  Both serving loops (the
+    server and the one-at-a-time baseline) run under it."""
+    was = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if was:
+            gc.enable()
+
+
 def serve_sequential(requests: list, open_loop: bool = True) -> dict:
     """Baseline: one request at a time through the reference-compatible synchronous
     entry points (cuSZp_compress / cuSZp_decompress), in arrival order.  Outputs are
     carved from one buffer allocated before the clock starts (as the batched server's
     arena is), so the comparison measures batching, not per-request allocation."""
+    with _gc_paused():
+        return _serve_sequential(requests, open_loop)
+
+
+def _serve_sequential(requests: list, open_loop: bool) -> dict:
     from .pycuSZp import cuSZp
     api = cuSZp()
     ordered = sorted(requests, key=lambda r: r.arrival)

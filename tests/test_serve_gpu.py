@@ -88,19 +88,6 @@ def test_resident_plans_are_reused_across_batches():
     srv.close()
 
 
-def test_arena_first_fit_merges_free_blocks():
-    from cuszp_b200.serve import Arena
-    a = Arena(4096, torch.device("cuda"))
-    x, y, z = a.alloc(1000), a.alloc(1000), a.alloc(1000)
-    assert (x, y, z) == (0, 1024, 2048) and a.alloc(2048) == -1
-    a.free(y, 1000)
-    a.free(x, 1000)
-    assert a.alloc(2048) == 0               # the two freed neighbours merged
-    a.free(0, 2048)
-    a.free(z, 1000)
-    assert a.used == 0 and a.starts == [0] and a.lens == [4096]
-
-
 def test_device_wait_timeout_is_raised_and_lane_recovers():
     """A launch whose bounded device wait gives up must not hand back a result: the lane's
     error word comes back with the sizes and the server raises the library's status
