@@ -148,7 +148,8 @@ class Arena:
 
 class _Lane:
     """One stream with its resident batch plans (one per (kind, dtype, dim) group), a
-    resident single-array workspace and size buffers; busy while a batch is on the GPU."""
+    resident single-array workspace, size and error words and completion events; busy
+    while any of its requests is on the GPU."""
 
     WS_BYTES = 1 << 20   # single-array workspace: arrays of up to ~131k tiles (512 MiB f32)
 
@@ -181,8 +182,10 @@ class _Lane:
         self.order: list = []
 
     def errors(self) -> list:
-        """(source, error word) per launch of the batch in flight; source None: the lane
-        workspace."""
+        """(source, error word) pairs to check; source None: the lane workspace.  For
+        single-array calls, the word copied after the next request not yet handed out
+        (the word is sticky, so it also covers every call before it); for a batch, one
+        word per plan it launched."""
         if self.direct:
             return [(None, self.words_c[2 * self.next] & 0xffffffff)]
         return [(h, self.err_c[i]) for i, h in enumerate(self.err_src)]
