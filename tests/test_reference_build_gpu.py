@@ -11,8 +11,8 @@ must be identical.  Both output buffers start zeroed: the reference leaves the
 Sizes: the 2^24-element f32 sinusoid field (plain, 1D) at full size, the
 uniform-with-zeros f64 field at 2048 x 2048 (fixed, 2D), the Gaussian random field
 at 128^3 (outlier, in all three processing dimensionalities), every dtype x
-mode x dim combination on a ragged 3D shape, and a 4 GiB f32 array (2^30 values) in
-each processing dimensionality.
+mode x dim combination on a ragged 3D shape, and 4 GiB arrays (2^30 f32 values, 2^29
+f64 values) in each processing dimensionality.
 """
 import ctypes
 import os
@@ -132,4 +132,15 @@ def field_4gib(cuda):
 def test_4gib_array(ref, field_4gib, dim, mode):
     S = _check(ref, field_4gib, 1e-3, mode, dim)
     assert S > (1 << 29)
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dim,mode", [(1, "outlier"), (2, "fixed"), (3, "plain")])
+def test_4gib_f64_array(ref, cuda, dim, mode):
+    """2^29 f64 values (4 GiB) as 512 x 1024 x 1024."""
+    from cuszp_b200 import datagen
+    x = datagen.sinusoid_field(1 << 29, seed=8, device=cuda, dtype=torch.float64).reshape(512, 1024, 1024)
+    S = _check(ref, x, 1e-3, mode, dim)
+    assert S > (1 << 28)
+    del x
     torch.cuda.empty_cache()
