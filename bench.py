@@ -522,7 +522,7 @@ def run_batched(device, count=4096, steps=5, seed=3):
 def run_serving(device, rates=(1000.0, 5000.0, 20000.0, 50000.0), count=1500, seed=4):
     """Serving form: open-loop Poisson arrivals, 70% compress / 30% decompress, 4 KiB-256 MiB
     log-uniform, 80% f32, modes uniform, 1D/2D/3D, abs eb log-uniform [1e-5, 1e-2], 64 GiB
-    budget; continuous batching against one-request-at-a-time calls."""
+    budget; the serving loop (cuszp_b200.serve) against one-request-at-a-time calls."""
     import dataclasses
     import gc
 

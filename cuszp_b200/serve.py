@@ -1,4 +1,4 @@
-"""Continuous-batching request loop for compress / decompress requests.
+"""Request-serving loop for compress / decompress requests.
 
 Requests of mixed size, dtype, mode and dimensionality arrive over time.  Each loop
 iteration
