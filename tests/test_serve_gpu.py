@@ -166,3 +166,32 @@ def test_serve_submit_matches_single_array_calls():
     assert st == 0
     done.synchronize()
     assert int(words[0]) == 0 and int(words[1]) == 0
+
+
+def test_request_beyond_the_lane_workspace_goes_out_as_a_plan():
+    """An array of more tiles than a lane's single-array workspace holds (2^29 + 2^20 f32
+    values: 131,328 tiles) is served as a batch of one through a plan, which has its own
+    workspace; stream and reconstruction equal the single-array calls'."""
+    from cuszp_b200 import codec, serve
+    n = (1 << 29) + (1 << 20)
+    g = torch.Generator(device="cuda").manual_seed(4)
+    x = torch.randn(n, generator=g, device="cuda").mul_(1e-3)
+    x.add_(torch.sin(torch.arange(n, device="cuda", dtype=torch.float32).mul_(1e-3)))
+    srv = serve.Server(budget_bytes=6 << 30, lanes=2, max_batch=4)
+    r = serve.Request(rid=0, kind="compress", dtype=torch.float32, mode="outlier", dim=1, dims=(0, 0, 0), eb=1e-3,
+                      data=x, n=n)
+    assert not srv._fits_lane_ws(r)
+    srv.run([r], open_loop=False)
+    assert srv.direct_calls == 0 and any(lane.plans for lane in srv.lanes)
+    ref = codec.compress(x, 1e-3, "outlier")
+    assert r.size == ref.numel() and torch.equal(r.result, ref)
+    d = serve.Request(rid=1, kind="decompress", dtype=torch.float32, mode="outlier", dim=1, dims=(0, 0, 0),
+                      eb=1e-3, data=ref, n=n)
+    srv.run([d], open_loop=False)
+    assert srv.direct_calls == 0
+    assert torch.equal(d.result, codec.decompress(ref, (n,), torch.float32, 1e-3, "outlier"))
+    srv.release(r)
+    srv.release(d)
+    srv.close()
+    del x, ref
+    torch.cuda.empty_cache()
