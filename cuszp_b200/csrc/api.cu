@@ -188,13 +188,8 @@ extern "C" int cuSZp_compress_async(const void* d_oriData, unsigned char* d_cmpB
     if (cmpCapacity < p.g.rate_bytes) return E_CAPACITY;   // the rate region alone does not fit
     p.g.cap = cmpCapacity;
     if (!d_workspace || workspaceBytes < workspace_bytes(p) || (uintptr_t)d_workspace % 16) return E_WORKSPACE;
-    if ((st = launch_compress(p, d_oriData, d_cmpBytes, (double)errorBound, d_workspace, stream))) return st;
-    if (d_cmpSize) {
-        const void* src = &reinterpret_cast<WsHeader*>(d_workspace)->total;
-        if (cudaMemcpyAsync(d_cmpSize, src, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
-            return E_CUDA;
-    }
-    return OK;
+    // the kernel's last CTA writes the length into d_cmpSize (no copy after the kernel)
+    return launch_compress(p, d_oriData, d_cmpBytes, (double)errorBound, d_workspace, stream, d_cmpSize);
 }
 
 extern "C" int cuSZp_decompress_async(void* d_decData, const unsigned char* d_cmpBytes, size_t nbEle,

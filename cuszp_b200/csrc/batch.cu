@@ -240,6 +240,7 @@ struct BatchTiles {
     unsigned long long* status;
     unsigned long long* sizes;
     __device__ __forceinline__ uint64_t total() const { return total_tiles; }
+    __device__ __forceinline__ unsigned long long* size_out() const { return nullptr; }   // per array: `sizes`
     // one tile per ticket: a group of tiles could straddle two arrays
     __device__ __forceinline__ int ticket_tiles() const { return 1; }
     __device__ __forceinline__ void locate(int64_t t, int32_t& a, int64_t& local) const

@@ -106,6 +106,8 @@ struct Geom {
     uint64_t cap;          // compress: bytes the stream buffer holds (~0: not checked); a
                            // payload span that would end past it is not written and
                            // ERR_CAPACITY is raised (the stream length is still computed)
+    unsigned long long* size_out;   // single-array compress: the CTA that finishes last
+                                    // writes the stream length here (null: not asked)
 };
 
 // Blocks per tensor-map box of the TMA kernels' grouped 2D maps (one codec warp's share
@@ -468,7 +470,11 @@ __device__ __forceinline__ uint64_t warp_lookback(unsigned long long* status, in
 }
 
 // Last CTA out resets the workspace so the next call finds it zeroed.
-__device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* status, uint64_t ntiles)
+// The CTA that finishes last resets the workspace for the next call and, when asked
+// (size_out), writes the stream length there: it is the last writer, so the length is
+// final, and no copy after the kernel is needed.
+__device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* status, uint64_t ntiles,
+                                           unsigned long long* size_out = nullptr)
 {
     __shared__ int s_last;
     __syncthreads();
@@ -486,6 +492,7 @@ __device__ __forceinline__ void finish_cta(WsHeader* hdr, unsigned long long* st
             hdr->done = 0u;
             // a stream length after a timed-out wait may be partial: mark it invalid
             if (timed_out(&hdr->err)) hdr->total = ~0ull;
+            if (size_out) *size_out = *reinterpret_cast<volatile unsigned long long*>(&hdr->total);
         }
         __threadfence();
     }

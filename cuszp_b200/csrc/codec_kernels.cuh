@@ -1029,7 +1029,7 @@ compress_kernel(const T* __restrict__ in, uint8_t* __restrict__ cmp, Geom g, T r
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SingleSource<T, DIM, MODE, Tl> src{in, cmp, g, recip, hdr, status, &hdr->total};
     compress_pipeline<T, DIM, Tl>(src, smem_raw, &hdr->err);
-    finish_cta(hdr, status, g.ntiles);
+    finish_cta(hdr, status, g.ntiles, g.size_out);
 }
 
 // --------------------------------------------------------------- decompress phases

@@ -433,9 +433,13 @@ static int launch(const Problem& p, bool comp, const void* a0, void* a1, double 
     return e == cudaSuccess ? OK : E_CUDA;
 }
 
-int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double eb, void* ws, cudaStream_t s)
+int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double eb, void* ws, cudaStream_t s,
+                    unsigned long long* d_size)
 {
-    return launch(p, true, d_in, d_cmp, eb, ws, s);
+    if (!d_size) return launch(p, true, d_in, d_cmp, eb, ws, s);
+    Problem q = p;
+    q.g.size_out = d_size;
+    return launch(q, true, d_in, d_cmp, eb, ws, s);
 }
 
 int launch_decompress(const Problem& p, void* d_out, const uint8_t* d_cmp, double eb, void* ws, cudaStream_t s)

@@ -45,7 +45,10 @@ size_t max_stream_bytes(const Problem& p);
 // workspace_bytes(p) (the kernels leave it zeroed again, except for the error
 // word and the stream length in the header).  eb is the absolute error bound
 // (float for f32, double for f64 -- the generic API widens a float).
-int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double eb, void* ws, cudaStream_t s);
+// d_size: when non-null, the kernel writes the stream length there (~0 after a
+// timed-out wait), as the workspace header's `total`.
+int launch_compress(const Problem& p, const void* d_in, uint8_t* d_cmp, double eb, void* ws, cudaStream_t s,
+                    unsigned long long* d_size = nullptr);
 int launch_decompress(const Problem& p, void* d_out, const uint8_t* d_cmp, double eb, void* ws, cudaStream_t s);
 
 // The TMA kernels: whether the environment allows them (CUSZP_NO_TMA=1 turns them

@@ -565,6 +565,7 @@ struct SingleTiles {
     unsigned long long* total_out;
     int tickets = 1;   // decompress: tiles per ticket (1 or up to kMaxTicketTiles)
     __device__ __forceinline__ uint64_t total() const { return g->ntiles; }
+    __device__ __forceinline__ unsigned long long* size_out() const { return g->size_out; }
     __device__ __forceinline__ int ticket_tiles() const { return tickets; }
     __device__ __forceinline__ void locate(int64_t t, int32_t& a, int64_t& local) const { a = 0; local = t; }
     __device__ __forceinline__ TileArray array(int32_t) const
@@ -888,7 +889,7 @@ __device__ __forceinline__ void compress_tma_body(const Src& src, WsHeader* __re
         }
         while (ok && q0.k >= 0) ok = pop();
     }
-    finish_cta(hdr, status_all, ntotal);
+    finish_cta(hdr, status_all, ntotal, src.size_out());
 }
 
 template <typename T, int DIM, int MODE>
